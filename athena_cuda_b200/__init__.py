@@ -1,0 +1,253 @@
+"""Python access to libathena_b200.so (the sm_100a 2D ideal-MHD CTU+CT step).
+
+A thin ctypes layer over the C ABI in ``include/athena_b200.h``; the compute
+runs in the CUDA library only.  Importing this module raises if the library has
+not been built (``python -m athena_cuda_b200.build``): there is no fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libathena_b200.so"
+NPLANES = 11
+PLANES = ("d", "M1", "M2", "M3", "E", "B1c", "B2c", "B3c", "B1i", "B2i", "B3i")
+NGHOST = 4
+
+FLUX_ROE, FLUX_HLLE = 0, 1
+BC_REFLECT, BC_OUTFLOW, BC_PERIODIC = 1, 2, 4
+
+
+class AthbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"athb error {code}: {msg}")
+        self.code = code
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("nx1", C.c_int), ("nx2", C.c_int),
+        ("x1min", C.c_double), ("x1max", C.c_double), ("x2min", C.c_double), ("x2max", C.c_double),
+        ("bc_ix1", C.c_int), ("bc_ox1", C.c_int), ("bc_ix2", C.c_int), ("bc_ox2", C.c_int),
+        ("gamma", C.c_double), ("cour_no", C.c_double), ("tlim", C.c_double),
+        ("nlim", C.c_int), ("flux", C.c_int), ("device", C.c_int),
+    ]
+
+
+class GridInfo(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("nx1", "nx2", "sx", "sy", "is_", "ie", "js", "je")] + [
+        (n, C.c_double) for n in ("dx1", "dx2", "x1_0", "x2_0")] + [
+        ("idisp", C.c_int), ("jdisp", C.c_int)] + [
+        (n, C.c_double) for n in ("gamma", "gamma_1", "gamma_2")]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libathena_b200.so (once); raise if it is missing."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is not built; run `python -m athena_cuda_b200.build`")
+        L = C.CDLL(str(LIB_PATH))
+        P, I, D = C.c_void_p, C.c_int, C.c_double
+        dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int)
+        sig = {
+            "athb_create": (I, [C.POINTER(Config), C.POINTER(P)]),
+            "athb_destroy": (None, [P]),
+            "athb_shape": (I, [P, ip, ip]),
+            "athb_upload": (I, [P, dp, D, D, I]),
+            "athb_download": (I, [P, dp, dp, dp, ip]),
+            "athb_set_bvals": (I, [P]),
+            "athb_new_dt": (I, [P, dp]),
+            "athb_run": (I, [P, I, ip]),
+            "athb_run_async": (I, [P, I]),
+            "athb_synchronize": (I, [P]),
+            "athb_status": (I, [P, dp, dp, ip, ip]),
+            "athb_stream": (P, [P]),
+            "athb_last_error": (C.c_char_p, []),
+            "athb_error_string": (C.c_char_p, [I]),
+            "athb_create_from_athinput": (I, [C.c_char_p, I, C.POINTER(C.c_char_p), C.c_char_p, C.POINTER(P)]),
+            "athb_cpaw2d_errors": (I, [P, dp]),
+            "athb_grid_info_of": (I, [P, C.POINTER(GridInfo)]),
+            "athb_params_open": (I, [C.c_char_p, C.POINTER(P)]),
+            "athb_params_override": (I, [P, C.c_char_p]),
+            "athb_params_getd": (I, [P, C.c_char_p, C.c_char_p, dp]),
+            "athb_params_geti": (I, [P, C.c_char_p, C.c_char_p, ip]),
+            "athb_params_close": (None, [P]),
+            "athb_config_from_params": (I, [P, C.POINTER(Config)]),
+            "athb_problem_generate": (I, [C.c_char_p, C.POINTER(GridInfo), P, dp]),
+            "athb_host_alloc": (P, [C.c_ulonglong]),
+            "athb_host_free": (None, [P]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype, f.argtypes = res, args
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise AthbError(rc, lib().athb_last_error().decode())
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Params:
+    """An athinput parameter file (reference src/par.c format)."""
+
+    def __init__(self, path: str | os.PathLike, overrides: list[str] = ()):
+        self._h = C.c_void_p()
+        _check(lib().athb_params_open(str(path).encode(), C.byref(self._h)))
+        for o in overrides:
+            _check(lib().athb_params_override(self._h, o.encode()))
+
+    def getd(self, block: str, name: str) -> float:
+        v = C.c_double()
+        _check(lib().athb_params_getd(self._h, block.encode(), name.encode(), C.byref(v)))
+        return v.value
+
+    def geti(self, block: str, name: str) -> int:
+        v = C.c_int()
+        _check(lib().athb_params_geti(self._h, block.encode(), name.encode(), C.byref(v)))
+        return v.value
+
+    def config(self) -> Config:
+        c = Config()
+        _check(lib().athb_config_from_params(self._h, C.byref(c)))
+        return c
+
+    def close(self) -> None:
+        if self._h:
+            lib().athb_params_close(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def grid_info(cfg: Config) -> GridInfo:
+    """Host-side geometry of a config (reference src/init_grid.c)."""
+    g = GridInfo()
+    g.nx1, g.nx2 = cfg.nx1, cfg.nx2
+    g.sx, g.sy = cfg.nx1 + 2 * NGHOST, cfg.nx2 + 2 * NGHOST
+    g.is_, g.js = NGHOST, NGHOST
+    g.ie, g.je = cfg.nx1 + NGHOST - 1, cfg.nx2 + NGHOST - 1
+    g.dx1 = (cfg.x1max - cfg.x1min) / cfg.nx1
+    g.dx2 = (cfg.x2max - cfg.x2min) / cfg.nx2
+    g.x1_0, g.x2_0 = cfg.x1min, cfg.x2min
+    g.idisp, g.jdisp = -NGHOST, -NGHOST
+    g.gamma, g.gamma_1, g.gamma_2 = cfg.gamma, cfg.gamma - 1.0, cfg.gamma - 2.0
+    return g
+
+
+def problem_state(name: str, params: Params) -> np.ndarray:
+    """Initial state of a built-in problem generator, as (11, sy, sx) planes."""
+    cfg = params.config()
+    g = grid_info(cfg)
+    planes = np.zeros((NPLANES, g.sy, g.sx))
+    _check(lib().athb_problem_generate(name.encode(), C.byref(g), params._h, _dp(planes)))
+    return planes
+
+
+class Grid:
+    """A device-resident grid (an ``athb_ctx``)."""
+
+    def __init__(self, handle: C.c_void_p):
+        self._h = handle
+        sx, sy = C.c_int(), C.c_int()
+        _check(lib().athb_shape(self._h, C.byref(sx), C.byref(sy)))
+        self.sx, self.sy = sx.value, sy.value
+
+    @classmethod
+    def create(cls, cfg: Config) -> "Grid":
+        h = C.c_void_p()
+        _check(lib().athb_create(C.byref(cfg), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_athinput(cls, path, problem: str, overrides: list[str] = ()) -> "Grid":
+        h = C.c_void_p()
+        arr = (C.c_char_p * max(1, len(overrides)))(*[o.encode() for o in overrides])
+        _check(lib().athb_create_from_athinput(str(path).encode(), len(overrides), arr,
+                                               problem.encode(), C.byref(h)))
+        return cls(h)
+
+    def upload(self, planes: np.ndarray, dt: float = 0.0, time: float = 0.0, nstep: int = 0) -> None:
+        planes = np.ascontiguousarray(planes, dtype=np.float64)
+        assert planes.shape == (NPLANES, self.sy, self.sx)
+        _check(lib().athb_upload(self._h, _dp(planes), dt, time, nstep))
+
+    def download(self) -> tuple[np.ndarray, float, float, int]:
+        planes = np.empty((NPLANES, self.sy, self.sx))
+        dt, t, n = C.c_double(), C.c_double(), C.c_int()
+        _check(lib().athb_download(self._h, _dp(planes), C.byref(dt), C.byref(t), C.byref(n)))
+        return planes, dt.value, t.value, n.value
+
+    def set_bvals(self) -> None:
+        _check(lib().athb_set_bvals(self._h))
+
+    def new_dt(self) -> float:
+        dt = C.c_double()
+        _check(lib().athb_new_dt(self._h, C.byref(dt)))
+        return dt.value
+
+    def run(self, nsteps: int) -> int:
+        done = C.c_int()
+        _check(lib().athb_run(self._h, nsteps, C.byref(done)))
+        return done.value
+
+    def run_async(self, nsteps: int) -> None:
+        _check(lib().athb_run_async(self._h, nsteps))
+
+    def synchronize(self) -> None:
+        _check(lib().athb_synchronize(self._h))
+
+    def status(self) -> dict:
+        t, dt, n, done = C.c_double(), C.c_double(), C.c_int(), C.c_int()
+        _check(lib().athb_status(self._h, C.byref(t), C.byref(dt), C.byref(n), C.byref(done)))
+        return {"time": t.value, "dt": dt.value, "nstep": n.value, "done": bool(done.value)}
+
+    @property
+    def stream(self) -> int:
+        return lib().athb_stream(self._h) or 0
+
+    def cpaw2d_errors(self) -> np.ndarray:
+        err = np.zeros(9)
+        _check(lib().athb_cpaw2d_errors(self._h, _dp(err)))
+        return err
+
+    def close(self) -> None:
+        if self._h:
+            lib().athb_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def write_athinput(path, blocks: dict) -> Path:
+    """Write an athinput file from {block: {name: value}} (reference format)."""
+    path = Path(path)
+    lines = []
+    for b, kv in blocks.items():
+        lines.append(f"<{b}>")
+        for k, v in kv.items():
+            lines.append(f"{k} = {v!r}" if isinstance(v, float) else f"{k} = {v}")
+        lines.append("")
+    path.write_text("\n".join(lines))
+    return path

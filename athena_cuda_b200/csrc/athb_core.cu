@@ -1,0 +1,508 @@
+// athb_core.cu -- device-resident context, step launch sequence, CUDA-graph
+// loop and the athb_* C ABI of libathena_b200.so.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "athb_internal.h"
+#include "step_kernels.cuh"
+
+using namespace athb;
+
+// ---------------------------------------------------------------------------
+// error reporting
+// ---------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+
+int athb_fail(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define CUDA_TRY(call)                                                                   \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return athb_fail(ATHB_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                       __FILE__, __LINE__);                                              \
+  } while (0)
+
+extern "C" const char* athb_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" const char* athb_error_string(int code) {
+  switch (code) {
+  case ATHB_OK: return "ok";
+  case ATHB_ERR_ARG: return "invalid argument";
+  case ATHB_ERR_CUDA: return "CUDA error";
+  case ATHB_ERR_STATE: return "non-finite state";
+  case ATHB_ERR_PARSE: return "parameter error";
+  case ATHB_ERR_NOMEM: return "out of memory";
+  case ATHB_ERR_NOTFOUND: return "not found";
+  default: return "unknown error";
+  }
+}
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+static GridArgs grid_args(const athb_ctx* c, int from) {
+  GridArgs g;
+  g.in = c->state[from];
+  g.out = c->state[from ^ 1];
+  g.scr = c->scr;
+  g.st = c->st;
+  g.ps = c->ps;
+  g.pitch = c->pitch;
+  g.is = c->is; g.ie = c->ie; g.js = c->js; g.je = c->je;
+  g.ly = c->ly;
+  g.dx1 = c->dx1; g.dx2 = c->dx2;
+  g.eos = Eos{c->cfg.gamma, c->cfg.gamma - 1.0, c->cfg.gamma - 2.0};
+  g.bc[0] = c->cfg.bc_ix1; g.bc[1] = c->cfg.bc_ox1; g.bc[2] = c->cfg.bc_ix2; g.bc[3] = c->cfg.bc_ox2;
+  return g;
+}
+
+static int blocks_for(long long n) { return (int)((n + kThreads - 1) / kThreads); }
+
+static bool valid_bc(int b) { return b == BC_REFLECT || b == BC_OUTFLOW || b == BC_PERIODIC; }
+
+int athb_ctx_validate(const athb_config* cfg) {
+  if (!cfg) return athb_fail(ATHB_ERR_ARG, "null config");
+  if (cfg->nx1 < 4 || cfg->nx2 < 4)
+    return athb_fail(ATHB_ERR_ARG, "grid must have Nx1 >= 4 and Nx2 >= 4 (got %d x %d)", cfg->nx1, cfg->nx2);
+  if ((long long)(cfg->nx1 + 8) * (cfg->nx2 + 8) > (1LL << 30))
+    return athb_fail(ATHB_ERR_ARG, "grid too large (%d x %d)", cfg->nx1, cfg->nx2);
+  if (!(cfg->x1max >= cfg->x1min) || !(cfg->x2max >= cfg->x2min))
+    return athb_fail(ATHB_ERR_ARG, "x1max < x1min or x2max < x2min");
+  if (!valid_bc(cfg->bc_ix1) || !valid_bc(cfg->bc_ox1) || !valid_bc(cfg->bc_ix2) || !valid_bc(cfg->bc_ox2))
+    return athb_fail(ATHB_ERR_ARG, "boundary flags must be 1 (reflect), 2 (outflow) or 4 (periodic)");
+  if (cfg->flux != ATHB_FLUX_ROE && cfg->flux != ATHB_FLUX_HLLE)
+    return athb_fail(ATHB_ERR_ARG, "unknown flux %d", cfg->flux);
+  if (!(cfg->gamma > 1.0)) return athb_fail(ATHB_ERR_ARG, "gamma must be > 1");
+  return ATHB_OK;
+}
+
+extern "C" int athb_create(const athb_config* cfg, athb_ctx** out) {
+  if (!out) return athb_fail(ATHB_ERR_ARG, "null output pointer");
+  *out = nullptr;
+  int rc = athb_ctx_validate(cfg);
+  if (rc) return rc;
+  athb_ctx* c = new (std::nothrow) athb_ctx();
+  if (!c) return athb_fail(ATHB_ERR_NOMEM, "context allocation failed");
+  c->cfg = *cfg;
+  c->sx = cfg->nx1 + 2 * kNghost;
+  c->sy = cfg->nx2 + 2 * kNghost;
+  c->pitch = (c->sx + 15) & ~15;
+  c->ps = (long long)c->pitch * c->sy;
+  c->is = kNghost; c->ie = cfg->nx1 + kNghost - 1;
+  c->js = kNghost; c->je = cfg->nx2 + kNghost - 1;
+  // src/init_grid.c: dx = (xmax - xmin)/Nx, x_0 = xmin, disp = -nghost
+  c->dx1 = (cfg->x1max - cfg->x1min) / (double)cfg->nx1;
+  c->dx2 = (cfg->x2max - cfg->x2min) / (double)cfg->nx2;
+  c->x1_0 = cfg->x1min; c->x2_0 = cfg->x2min;
+  {
+    long long cols = cfg->nx1 + 4, faces = cfg->nx2 + 3;
+    long long ly = (cols * faces) / (148LL * 512);
+    c->ly = (int)std::max(4LL, std::min(64LL, ly));
+  }
+  cudaError_t e = cudaSetDevice(cfg->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  const size_t state_bytes = sizeof(double) * (size_t)c->ps * NSTATE;
+  const size_t scr_bytes = sizeof(double) * (size_t)c->ps * NSCRATCH;
+  if (e == cudaSuccess) e = cudaMalloc(&c->state[0], state_bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&c->state[1], state_bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&c->scr, scr_bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&c->st, sizeof(StepState));
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->state[0], 0, state_bytes, c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->state[1], 0, state_bytes, c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->scr, 0, scr_bytes, c->stream);
+  if (e == cudaSuccess) {
+    StepState h{};
+    h.tlim = cfg->tlim;
+    h.cour_no = cfg->cour_no;
+    h.nlim = cfg->nlim;
+    e = cudaMemcpyAsync(c->st, &h, sizeof h, cudaMemcpyHostToDevice, c->stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) {
+    athb_destroy(c);
+    return athb_fail(e == cudaErrorMemoryAllocation ? ATHB_ERR_NOMEM : ATHB_ERR_CUDA,
+                     "athb_create: %s", cudaGetErrorString(e));
+  }
+  *out = c;
+  return ATHB_OK;
+}
+
+static void drop_graphs(athb_ctx* c) {
+  for (int k = 0; k < 2; k++)
+    if (c->graph[k]) { cudaGraphExecDestroy(c->graph[k]); c->graph[k] = nullptr; }
+}
+
+extern "C" void athb_destroy(athb_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->cfg.device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  drop_graphs(c);
+  cudaFree(c->state[0]);
+  cudaFree(c->state[1]);
+  cudaFree(c->scr);
+  cudaFree(c->st);
+  cudaFree(c->aos);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+extern "C" int athb_shape(const athb_ctx* c, int* sx, int* sy) {
+  if (!c) return athb_fail(ATHB_ERR_ARG, "null context");
+  if (sx) *sx = c->sx;
+  if (sy) *sy = c->sy;
+  return ATHB_OK;
+}
+
+extern "C" void* athb_stream(athb_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+extern "C" void* athb_host_alloc(unsigned long long bytes) {
+  void* p = nullptr;
+  if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) return nullptr;
+  return p;
+}
+extern "C" void athb_host_free(void* p) { if (p) cudaFreeHost(p); }
+
+// ---------------------------------------------------------------------------
+// state transfer
+// ---------------------------------------------------------------------------
+int athb_set_clock(athb_ctx* c, double dt, double time, int nstep) {
+  StepState h{};
+  h.dt = dt;
+  h.time = time;
+  h.tlim = c->cfg.tlim;
+  h.cour_no = c->cfg.cour_no;
+  h.nstep = nstep;
+  h.nlim = c->cfg.nlim;
+  h.done = !((time < c->cfg.tlim) && (c->cfg.nlim < 0 || nstep < c->cfg.nlim));
+  h.dtodx1 = dt / c->dx1;
+  h.dtodx2 = dt / c->dx2;
+  h.hdtodx1 = 0.5 * h.dtodx1;
+  h.hdtodx2 = 0.5 * h.dtodx2;
+  h.hdt = 0.5 * dt;
+  CUDA_TRY(cudaMemcpyAsync(c->st, &h, sizeof h, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return ATHB_OK;
+}
+
+int athb_read_clock(athb_ctx* c, StepState* h) {
+  CUDA_TRY(cudaMemcpyAsync(h, c->st, sizeof *h, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return ATHB_OK;
+}
+
+extern "C" int athb_upload(athb_ctx* c, const double* planes, double dt, double time, int nstep) {
+  if (!c || !planes) return athb_fail(ATHB_ERR_ARG, "null argument");
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  CUDA_TRY(cudaMemcpy2DAsync(c->state[c->cur], sizeof(double) * c->pitch, planes,
+                             sizeof(double) * c->sx, sizeof(double) * c->sx,
+                             (size_t)c->sy * NSTATE, cudaMemcpyHostToDevice, c->stream));
+  return athb_set_clock(c, dt, time, nstep);
+}
+
+extern "C" int athb_download(athb_ctx* c, double* planes, double* dt, double* time, int* nstep) {
+  if (!c) return athb_fail(ATHB_ERR_ARG, "null context");
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  if (planes)
+    CUDA_TRY(cudaMemcpy2DAsync(planes, sizeof(double) * c->sx, c->state[c->cur],
+                               sizeof(double) * c->pitch, sizeof(double) * c->sx,
+                               (size_t)c->sy * NSTATE, cudaMemcpyDeviceToHost, c->stream));
+  StepState h;
+  int rc = athb_read_clock(c, &h);
+  if (rc) return rc;
+  if (dt) *dt = h.dt;
+  if (time) *time = h.time;
+  if (nstep) *nstep = h.nstep;
+  return ATHB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// launch sequences
+// ---------------------------------------------------------------------------
+int athb_launch_ghost_phase(athb_ctx* c, int buf, int mode, int sides) {
+  GridArgs g = grid_args(c, buf ^ 1);  // out = buf
+  const int nframe = c->js * c->sx + (c->sy - c->je - 1) * c->sx + c->cfg.nx2 * 2 * c->is;
+  k_ghost<<<blocks_for(nframe), kThreads, 0, c->stream>>>(g, c->sx, c->sy, nframe, mode, sides);
+  CUDA_TRY(cudaGetLastError());
+  return ATHB_OK;
+}
+
+int athb_launch_ghost(athb_ctx* c, int buf) { return athb_launch_ghost_phase(c, buf, 3, 3); }
+
+int athb_launch_set_dt(athb_ctx* c, double dt) {
+  k_set_dt<<<1, 1, 0, c->stream>>>(c->st, dt, c->dx1, c->dx2);
+  CUDA_TRY(cudaGetLastError());
+  return ATHB_OK;
+}
+
+int athb_launch_cfl(athb_ctx* c, int buf) {
+  GridArgs g = grid_args(c, buf);
+  const int n = c->cfg.nx1 * c->cfg.nx2;
+  k_cfl<<<blocks_for(n), kThreads, 0, c->stream>>>(g, c->cfg.nx1, n);
+  CUDA_TRY(cudaGetLastError());
+  return ATHB_OK;
+}
+
+// The integrator proper: reads state[from], writes the interior of state[from^1].
+// With ev != nullptr, events ev[0..5] bracket the five kernels.
+int athb_launch_integrate_split(athb_ctx* c, int from, cudaEvent_t* ev) {
+#define MARK(k) do { if (ev) CUDA_TRY(cudaEventRecord(ev[k], c->stream)); } while (0)
+  GridArgs g = grid_args(c, from);
+  const int nx1 = c->cfg.nx1, nx2 = c->cfg.nx2;
+  PredictGeom pg;
+  pg.xseg = (nx1 + 3 + kXFacesPerWarp - 1) / kXFacesPerWarp;   // faces [is-1, ie+2]
+  pg.xrowblk = (nx2 + 4 + kXRowsPerBlock - 1) / kXRowsPerBlock;  // rows [js-2, je+2]
+  pg.nx_blocks = pg.xseg * pg.xrowblk;
+  pg.ycolblk = (nx1 + 4 + kThreads - 1) / kThreads;             // columns [is-2, ie+2]
+  pg.yseg = (nx2 + 3 + c->ly - 1) / c->ly;                      // faces [js-1, je+2]
+  pg.ny_blocks = pg.ycolblk * pg.yseg;
+  MARK(0);
+  if (c->cfg.flux == ATHB_FLUX_HLLE)
+    k_predict<kFluxHlle><<<pg.nx_blocks + pg.ny_blocks, kThreads, 0, c->stream>>>(g, pg);
+  else
+    k_predict<kFluxRoe><<<pg.nx_blocks + pg.ny_blocks, kThreads, 0, c->stream>>>(g, pg);
+  CUDA_TRY(cudaGetLastError());
+
+  MARK(1);
+  k_emf<<<blocks_for((long long)(nx1 + 3) * (nx2 + 3)), kThreads, 0, c->stream>>>(
+      g, c->is - 1, c->js - 1, nx1 + 3, nx2 + 3, S_FX, S_FY);
+  CUDA_TRY(cudaGetLastError());
+
+  CorrectGeom cg;
+  cg.xw = nx1 + 1; cg.xn = nx2 + 3;
+  cg.yw = nx1 + 3; cg.yn = nx2 + 1;
+  cg.ew = nx1 + 3; cg.en = nx2 + 3;
+  cg.xb = blocks_for((long long)cg.xw * cg.xn);
+  cg.yb = blocks_for((long long)cg.yw * cg.yn);
+  cg.eb = blocks_for((long long)cg.ew * cg.en);
+  MARK(2);
+  if (c->cfg.flux == ATHB_FLUX_HLLE)
+    k_correct<kFluxHlle><<<cg.xb + cg.yb + cg.eb, kThreads, 0, c->stream>>>(g, cg);
+  else
+    k_correct<kFluxRoe><<<cg.xb + cg.yb + cg.eb, kThreads, 0, c->stream>>>(g, cg);
+  CUDA_TRY(cudaGetLastError());
+
+  MARK(3);
+  k_emf<<<blocks_for((long long)(nx1 + 1) * (nx2 + 1)), kThreads, 0, c->stream>>>(
+      g, c->is, c->js, nx1 + 1, nx2 + 1, S_FX2, S_FY2);
+  CUDA_TRY(cudaGetLastError());
+
+  MARK(4);
+  const int n = nx1 * nx2;
+  k_update<<<blocks_for(n), kThreads, 0, c->stream>>>(g, nx1, n);
+  CUDA_TRY(cudaGetLastError());
+  MARK(5);
+  return ATHB_OK;
+#undef MARK
+}
+
+int athb_launch_integrate(athb_ctx* c, int from) { return athb_launch_integrate_split(c, from, nullptr); }
+
+// Per-kernel timing of the loop step (CUDA events on the context's stream
+// between consecutive launches).  Kernel order: predict, emf(half), correct,
+// emf(full), update, finalize, ghost.
+extern "C" int athb_profile_steps(athb_ctx* c, int nsteps, double* ms_out) {
+  if (!c || nsteps < 1 || !ms_out) return athb_fail(ATHB_ERR_ARG, "bad arguments");
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  constexpr int K = 7;
+  std::vector<cudaEvent_t> ev((size_t)nsteps * (K + 1));
+  for (auto& e : ev) CUDA_TRY(cudaEventCreate(&e));
+  for (int k = 0; k < K; k++) ms_out[k] = 0.0;
+  int rc = ATHB_OK;
+  for (int s = 0; s < nsteps && rc == ATHB_OK; s++) {
+    cudaEvent_t* e = &ev[(size_t)s * (K + 1)];
+    const int from = c->cur;
+    GridArgs g = grid_args(c, from);
+    const int nx1 = c->cfg.nx1, nx2 = c->cfg.nx2;
+    rc = athb_launch_integrate_split(c, from, e);
+    if (rc) break;
+    k_finalize<<<1, 1, 0, c->stream>>>(c->st, c->dx1, c->dx2, 1);
+    CUDA_TRY(cudaEventRecord(e[6], c->stream));
+    rc = athb_launch_ghost(c, from ^ 1);
+    CUDA_TRY(cudaEventRecord(e[7], c->stream));
+    c->cur ^= 1;
+    (void)g; (void)nx1; (void)nx2;
+  }
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  for (int s = 0; s < nsteps && rc == ATHB_OK; s++) {
+    cudaEvent_t* e = &ev[(size_t)s * (K + 1)];
+    for (int k = 0; k < K; k++) {
+      float ms = 0.f;
+      CUDA_TRY(cudaEventElapsedTime(&ms, e[k], e[k + 1]));
+      ms_out[k] += ms;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  for (int k = 0; k < K; k++) ms_out[k] /= nsteps;
+  return rc;
+}
+
+// One iteration of the reference main loop (src/main.c:229-307) on the device.
+static int launch_loop_step(athb_ctx* c, int from) {
+  int rc = athb_launch_integrate(c, from);
+  if (rc) return rc;
+  k_finalize<<<1, 1, 0, c->stream>>>(c->st, c->dx1, c->dx2, 1);
+  CUDA_TRY(cudaGetLastError());
+  return athb_launch_ghost(c, from ^ 1);
+}
+
+static int build_graph(athb_ctx* c, int from) {
+  cudaGraph_t graph = nullptr;
+  CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = launch_loop_step(c, from);
+  if (rc == ATHB_OK) rc = launch_loop_step(c, from ^ 1);
+  cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+  if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+  if (e != cudaSuccess) return athb_fail(ATHB_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&c->graph[from], graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return athb_fail(ATHB_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+  return ATHB_OK;
+}
+
+extern "C" int athb_run_async(athb_ctx* c, int nsteps) {
+  if (!c || nsteps < 0) return athb_fail(ATHB_ERR_ARG, "bad arguments");
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  int left = nsteps;
+  while (left >= 2) {
+    if (!c->graph[c->cur]) { int rc = build_graph(c, c->cur); if (rc) return rc; }
+    CUDA_TRY(cudaGraphLaunch(c->graph[c->cur], c->stream));
+    left -= 2;  // two steps: the state returns to the same buffer
+  }
+  if (left == 1) {
+    int rc = launch_loop_step(c, c->cur);
+    if (rc) return rc;
+    c->cur ^= 1;
+  }
+  return ATHB_OK;
+}
+
+extern "C" int athb_synchronize(athb_ctx* c) {
+  if (!c) return athb_fail(ATHB_ERR_ARG, "null context");
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return ATHB_OK;
+}
+
+extern "C" int athb_status(athb_ctx* c, double* time, double* dt, int* nstep, int* done) {
+  if (!c) return athb_fail(ATHB_ERR_ARG, "null context");
+  StepState h;
+  int rc = athb_read_clock(c, &h);
+  if (rc) return rc;
+  if (time) *time = h.time;
+  if (dt) *dt = h.dt;
+  if (nstep) *nstep = h.nstep;
+  if (done) *done = h.done;
+  if (h.flags & kErrNonFinite)
+    return athb_fail(ATHB_ERR_STATE, "non-finite or negative CFL rate at step %d", h.nstep);
+  return ATHB_OK;
+}
+
+extern "C" int athb_run(athb_ctx* c, int nsteps, int* steps_done) {
+  if (!c) return athb_fail(ATHB_ERR_ARG, "null context");
+  StepState before;
+  int rc = athb_read_clock(c, &before);
+  if (rc) return rc;
+  rc = athb_run_async(c, nsteps);
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  int nstep = 0;
+  rc = athb_status(c, nullptr, nullptr, &nstep, nullptr);
+  if (steps_done) *steps_done = nstep - before.nstep;
+  return rc;
+}
+
+extern "C" int athb_set_bvals(athb_ctx* c) {
+  if (!c) return athb_fail(ATHB_ERR_ARG, "null context");
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  int rc = athb_launch_ghost(c, c->cur);
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return ATHB_OK;
+}
+
+extern "C" int athb_new_dt(athb_ctx* c, double* dt) {
+  if (!c) return athb_fail(ATHB_ERR_ARG, "null context");
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  int rc = athb_launch_cfl(c, c->cur);
+  if (rc) return rc;
+  k_finalize<<<1, 1, 0, c->stream>>>(c->st, c->dx1, c->dx2, 0);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return athb_status(c, nullptr, dt, nullptr, nullptr);
+}
+
+extern "C" int athb_grid_info_of(const athb_ctx* c, athb_grid_info* g) {
+  if (!c || !g) return athb_fail(ATHB_ERR_ARG, "null argument");
+  g->nx1 = c->cfg.nx1; g->nx2 = c->cfg.nx2; g->sx = c->sx; g->sy = c->sy;
+  g->is = c->is; g->ie = c->ie; g->js = c->js; g->je = c->je;
+  g->dx1 = c->dx1; g->dx2 = c->dx2; g->x1_0 = c->x1_0; g->x2_0 = c->x2_0;
+  g->idisp = -c->is; g->jdisp = -c->js;
+  g->gamma = c->cfg.gamma; g->gamma_1 = c->cfg.gamma - 1.0; g->gamma_2 = c->cfg.gamma - 2.0;
+  return ATHB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 issue-rate probe: every thread runs 8 independent chains of dependent
+// DADD/DMUL pairs; 2 operations per pair.  All accesses stay in registers;
+// one store per thread keeps the work alive.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_fp64_probe(double* out, int iters, double a, double b) {
+  double x[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) x[k] = threadIdx.x * 1e-3 + k;
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      x[k] = __dadd_rn(x[k], a);
+      x[k] = __dmul_rn(x[k], b);
+    }
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) s += x[k];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+extern "C" int athb_fp64_peak(int device, double* ops_per_s) {
+  if (!ops_per_s) return athb_fail(ATHB_ERR_ARG, "null argument");
+  CUDA_TRY(cudaSetDevice(device));
+  int sms = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  const int blocks = sms * 8, threads = 256, iters = 4096;
+  double* out = nullptr;
+  CUDA_TRY(cudaMalloc(&out, sizeof(double) * blocks * threads));
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  double best = 0.0;
+  for (int rep = 0; rep < 6; rep++) {
+    CUDA_TRY(cudaEventRecord(e0));
+    k_fp64_probe<<<blocks, threads>>>(out, iters, 1.0000001, 0.9999999);
+    CUDA_TRY(cudaEventRecord(e1));
+    CUDA_TRY(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+    const double ops = 2.0 * 8.0 * iters * (double)blocks * threads;
+    if (rep > 0 && ms > 0.f) best = std::max(best, ops / (ms * 1e-3));
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  *ops_per_s = best;
+  return ATHB_OK;
+}

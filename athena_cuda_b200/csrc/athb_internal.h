@@ -1,0 +1,43 @@
+// athb_internal.h -- shared between the translation units of libathena_b200.so.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "../../include/athena_b200.h"
+
+namespace athb {
+struct StepState;
+constexpr int kNghost = 4;  // nghost, src/defs.h:82
+}  // namespace athb
+
+struct athb_ctx {
+  athb_config cfg;
+  int sx = 0, sy = 0, pitch = 0;  // padded host extents and device row pitch
+  long long ps = 0;               // device plane stride (doubles)
+  int is = 0, ie = 0, js = 0, je = 0;
+  int ly = 4;                     // y-sweep march segment length
+  double dx1 = 0, dx2 = 0, x1_0 = 0, x2_0 = 0;
+  double* state[2] = {nullptr, nullptr};  // double-buffered state planes
+  int cur = 0;                            // buffer holding the current state
+  double* scr = nullptr;                  // scratch planes
+  athb::StepState* st = nullptr;          // device time-stepping state
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // two-step loop, per parity
+  // drop-in staging: AoS copy of the host Gas array
+  void* aos = nullptr;
+  size_t aos_bytes = 0;
+  // cpaw2d reference solution (host copy of the initial cell-centred state)
+  double* cpaw_soln = nullptr;
+  ~athb_ctx() { delete[] cpaw_soln; }
+};
+
+// internal helpers (athb_core.cu)
+int athb_fail(int code, const char* fmt, ...);
+int athb_ctx_validate(const athb_config* cfg);
+int athb_set_clock(athb_ctx* c, double dt, double time, int nstep);
+int athb_launch_integrate(athb_ctx* c, int from);
+int athb_launch_integrate_split(athb_ctx* c, int from, cudaEvent_t* ev);
+int athb_launch_ghost(athb_ctx* c, int buf);
+int athb_launch_ghost_phase(athb_ctx* c, int buf, int mode, int sides);
+int athb_launch_cfl(athb_ctx* c, int buf);
+int athb_launch_set_dt(athb_ctx* c, double dt);

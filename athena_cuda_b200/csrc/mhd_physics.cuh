@@ -1,0 +1,761 @@
+// mhd_physics.cuh -- per-cell / per-face physics of the 2D adiabatic ideal-MHD
+// CTU step, written for FP64 SIMT on sm_100a.
+//
+// Every function here reproduces, operation for operation, the IEEE-754
+// binary64 arithmetic of the reference CPU path (same operands, same
+// association, same branch tests) so that a kernel built with --fmad=false is
+// bit-identical to it.  What differs is the shape of the work:
+//   * eigenmatrices are never materialised as dense 7x7 arrays: only the
+//     structurally non-zero entries are formed, and products whose factor is an
+//     exact 0.0 in the reference are skipped (x + (+-0) == x for every finite x,
+//     so sums over the remaining terms, kept in the reference order, are
+//     unchanged; only the sign of an exact zero result can differ);
+//   * entries that the reference defines as exact negations / copies of other
+//     entries reuse one product (-(a*b) == (-a)*b exactly in IEEE-754);
+//   * eigenvalues are formed first and the Roe solver returns the upwind flux
+//     before any eigenvector work when the face is supersonic.
+//
+// The functions are __host__ __device__ so the very same source can be checked
+// on a CPU against the reference routines; on the device they are inlined into
+// the step kernels.
+//
+// Reference sources restated (paths within the reference project):
+//   src/convert_var.c:37-95      Cons1D_to_Prim1D / Prim1D_to_Cons1D
+//   src/esystem_prim.c:36-235    esys_prim_adb_mhd   (eigensystem in primitives)
+//   src/lr_states_plm.c:64-248   lr_states           (characteristic PLM)
+//   src/esystem_roe.c:56-293     esys_roe_adb_mhd    (Roe-matrix eigensystem)
+//   src/flux_roe.c:54-259        flux_roe            (with HLLE fallback)
+//   src/flux_hlle.c:60-199       flux_hlle
+#pragma once
+
+#include <math.h>
+
+#if defined(__CUDACC__)
+#define ATHB_HD __host__ __device__ __forceinline__
+#else
+#define ATHB_HD static inline
+#endif
+
+namespace athb {
+
+constexpr double kTiny = 1.0e-20;   // TINY_NUMBER, src/defs.h:100
+
+// Conserved / primitive variables of one 1D slice, in the slice frame
+// (x = sweep direction).  Field order is that of Cons1D / Prim1D
+// (src/athena.h:75-98).
+struct Cons1 { double d, mx, my, mz, e, by, bz; };
+struct Prim1 { double d, vx, vy, vz, p, by, bz; };
+
+// Equation-of-state constants (the reference globals Gamma, Gamma_1, Gamma_2).
+struct Eos { double gamma, gamma_1, gamma_2; };
+
+// MAX / MIN / SIGN exactly as the reference macros (src/defs.h:87-94).
+ATHB_HD double rmax(double a, double b) { return (a > b) ? a : b; }
+ATHB_HD double rmin(double a, double b) { return (a < b) ? a : b; }
+ATHB_HD double rsign(double a) { return (a < 0.) ? -1. : 1.; }
+
+ATHB_HD double cget(const Cons1& u, int n) {
+  return n == 0 ? u.d : n == 1 ? u.mx : n == 2 ? u.my : n == 3 ? u.mz : n == 4 ? u.e : n == 5 ? u.by : u.bz;
+}
+
+// --- src/convert_var.c:37-55 -------------------------------------------------
+ATHB_HD Prim1 cons_to_prim(const Cons1& u, double bx, const Eos& eos) {
+  Prim1 w;
+  const double di = 1.0 / u.d;
+  w.d = u.d;
+  w.vx = u.mx * di;
+  w.vy = u.my * di;
+  w.vz = u.mz * di;
+  double p = u.e - 0.5 * (u.mx * u.mx + u.my * u.my + u.mz * u.mz) * di;
+  p -= 0.5 * (bx * bx + u.by * u.by + u.bz * u.bz);
+  p *= eos.gamma_1;
+  w.p = rmax(p, kTiny);
+  w.by = u.by;
+  w.bz = u.bz;
+  return w;
+}
+
+// --- src/convert_var.c:64-92 -------------------------------------------------
+ATHB_HD Cons1 prim_to_cons(const Prim1& w, double bx, const Eos& eos) {
+  Cons1 u;
+  u.d = w.d;
+  u.mx = w.d * w.vx;
+  u.my = w.d * w.vy;
+  u.mz = w.d * w.vz;
+  u.e = w.p / eos.gamma_1 + 0.5 * w.d * (w.vx * w.vx + w.vy * w.vy + w.vz * w.vz);
+  u.e += 0.5 * (bx * bx + w.by * w.by + w.bz * w.bz);
+  u.by = w.by;
+  u.bz = w.bz;
+  return u;
+}
+
+// ---------------------------------------------------------------------------
+// Primitive-variable eigensystem (src/esystem_prim.c:36-235), kept as the few
+// distinct scalars the 7x7 matrices are built from.
+//   Right eigenvectors (columns) R[row][col]:
+//     row0: R00=d*af  R02=d*as  R03=1  R04=R02  R06=R00
+//     row1: R10=-cf*af R12=-cs*as R14=-R12 R16=-R10
+//     row2: R20=qs*b2 R21=-b3 R22=-qf*b2 R24=-R22 R25=b3 R26=-R20
+//     row3: R30=qs*b3 R31=b2  R32=-qf*b3 R34=-R32 R35=-b2 R36=-R30
+//     row4: R40=d*asq*af R42=d*asq*as R44=R42 R46=R40
+//     row5: R50=as*b2 R51=-b3*s*sqrtd R52=-af*b2 R54=R52 R55=R51 R56=R50
+//     row6: R60=as*b3 R61=b2*s*sqrtd  R62=-af*b3 R64=R62 R65=R61 R66=R60
+//   Left eigenvectors (rows) L[row][col]:
+//     row0: L01..L06 ; row1: L12 L13 L15 L16 ; row2: L21..L26 ;
+//     row3: L30=1 L34=-1/asq ; row4 = (-L21,-L22,-L23, L24,L25,L26) ;
+//     row5 = (-L12,-L13, L15,L16) ; row6 = (-L01,-L02,-L03, L04,L05,L06)
+// ---------------------------------------------------------------------------
+struct PrimEig {
+  double ev[7];
+  double R00, R02, R10, R12, R20, R21, R22, R30, R31, R32, R40, R42, R50, R51, R52, R60, R61, R62;
+  double L01, L02, L03, L04, L05, L06, L12, L13, L15, L16, L21, L22, L23, L24, L25, L26, L34;
+};
+
+ATHB_HD void esys_prim(double d, double v1, double p, double b1, double b2, double b3,
+                       const Eos& eos, PrimEig& E) {
+  const double di = 1.0 / d;
+  const double btsq = b2 * b2 + b3 * b3;
+  const double vaxsq = b1 * b1 * di;
+  const double asq = eos.gamma * p * di;
+
+  const double ct2 = btsq * di;
+  const double tsum = vaxsq + ct2 + asq;
+  const double tdif = vaxsq + ct2 - asq;
+  const double cf2_cs2 = sqrt(tdif * tdif + 4.0 * asq * ct2);
+  const double cfsq = 0.5 * (tsum + cf2_cs2);
+  const double cf = sqrt(cfsq);
+  const double cssq = asq * vaxsq / cfsq;
+  const double cs = sqrt(cssq);
+
+  const double bt = sqrt(btsq);
+  double bet2, bet3;
+  if (bt == 0.0) { bet2 = 1.0; bet3 = 0.0; } else { bet2 = b2 / bt; bet3 = b3 / bt; }
+
+  double alpha_f, alpha_s;
+  if (cf2_cs2 == 0.0) { alpha_f = 1.0; alpha_s = 0.0; }
+  else if ((asq - cssq) <= 0.0) { alpha_f = 0.0; alpha_s = 1.0; }
+  else if ((cfsq - asq) <= 0.0) { alpha_f = 1.0; alpha_s = 0.0; }
+  else { alpha_f = sqrt((asq - cssq) / cf2_cs2); alpha_s = sqrt((cfsq - asq) / cf2_cs2); }
+
+  const double sqrtd = sqrt(d);
+  const double s = rsign(b1);
+  const double a = sqrt(asq);
+  double qf = cf * alpha_f * s;
+  double qs = cs * alpha_s * s;
+  const double af = a * alpha_f * sqrtd;
+  const double as = a * alpha_s * sqrtd;
+
+  const double vax = sqrt(vaxsq);
+  E.ev[0] = v1 - cf; E.ev[1] = v1 - vax; E.ev[2] = v1 - cs; E.ev[3] = v1;
+  E.ev[4] = v1 + cs; E.ev[5] = v1 + vax; E.ev[6] = v1 + cf;
+
+  E.R00 = d * alpha_f;        E.R02 = d * alpha_s;
+  E.R10 = -cf * alpha_f;      E.R12 = -cs * alpha_s;
+  E.R20 = qs * bet2;          E.R21 = -bet3;      E.R22 = -qf * bet2;
+  E.R30 = qs * bet3;          E.R31 = bet2;       E.R32 = -qf * bet3;
+  E.R40 = d * asq * alpha_f;  E.R42 = d * asq * alpha_s;
+  E.R50 = as * bet2;          E.R51 = -bet3 * s * sqrtd;  E.R52 = -af * bet2;
+  E.R60 = as * bet3;          E.R61 = bet2 * s * sqrtd;   E.R62 = -af * bet3;
+
+  const double na = 0.5 / asq;
+  qf = na * qf;
+  qs = na * qs;
+  const double af_prime = na * af * di;
+  const double as_prime = na * as * di;
+
+  E.L01 = -na * cf * alpha_f; E.L02 = qs * bet2; E.L03 = qs * bet3;
+  E.L04 = na * alpha_f * di;  E.L05 = as_prime * bet2; E.L06 = as_prime * bet3;
+  E.L12 = -0.5 * bet3; E.L13 = 0.5 * bet2;
+  E.L15 = -0.5 * bet3 * s / sqrtd; E.L16 = 0.5 * bet2 * s / sqrtd;
+  E.L21 = -na * cs * alpha_s; E.L22 = -qf * bet2; E.L23 = -qf * bet3;
+  E.L24 = na * alpha_s * di;  E.L25 = -af_prime * bet2; E.L26 = -af_prime * bet3;
+  E.L34 = -1.0 / asq;
+}
+
+// a = L * v for the primitive eigensystem, terms in the reference's column
+// order (src/lr_states_plm.c:122-133), exact zeros skipped.
+ATHB_HD void prim_project(const PrimEig& E, const double v[7], double a[7]) {
+  const double p01 = E.L01 * v[1], p02 = E.L02 * v[2], p03 = E.L03 * v[3];
+  const double p04 = E.L04 * v[4], p05 = E.L05 * v[5], p06 = E.L06 * v[6];
+  a[0] = p01 + p02 + p03 + p04 + p05 + p06;
+  a[6] = -p01 - p02 - p03 + p04 + p05 + p06;
+  const double p12 = E.L12 * v[2], p13 = E.L13 * v[3], p15 = E.L15 * v[5], p16 = E.L16 * v[6];
+  a[1] = p12 + p13 + p15 + p16;
+  a[5] = -p12 - p13 + p15 + p16;
+  const double p21 = E.L21 * v[1], p22 = E.L22 * v[2], p23 = E.L23 * v[3];
+  const double p24 = E.L24 * v[4], p25 = E.L25 * v[5], p26 = E.L26 * v[6];
+  a[2] = p21 + p22 + p23 + p24 + p25 + p26;
+  a[4] = -p21 - p22 - p23 + p24 + p25 + p26;
+  a[3] = v[0] + E.L34 * v[4];
+}
+
+// One left eigenvector of the primitive system, as 7 coefficients (for the
+// characteristic tracing loop, src/lr_states_plm.c:201-224).
+ATHB_HD void prim_left_row(const PrimEig& E, int n, double l[7]) {
+  for (int m = 0; m < 7; m++) l[m] = 0.0;
+  switch (n) {
+  case 0: l[1] = E.L01; l[2] = E.L02; l[3] = E.L03; l[4] = E.L04; l[5] = E.L05; l[6] = E.L06; break;
+  case 1: l[2] = E.L12; l[3] = E.L13; l[5] = E.L15; l[6] = E.L16; break;
+  case 2: l[1] = E.L21; l[2] = E.L22; l[3] = E.L23; l[4] = E.L24; l[5] = E.L25; l[6] = E.L26; break;
+  case 3: l[0] = 1.0; l[4] = E.L34; break;
+  case 4: l[1] = -E.L21; l[2] = -E.L22; l[3] = -E.L23; l[4] = E.L24; l[5] = E.L25; l[6] = E.L26; break;
+  case 5: l[2] = -E.L12; l[3] = -E.L13; l[5] = E.L15; l[6] = E.L16; break;
+  default: l[1] = -E.L01; l[2] = -E.L02; l[3] = -E.L03; l[4] = E.L04; l[5] = E.L05; l[6] = E.L06; break;
+  }
+}
+
+// One right eigenvector (column n) of the primitive system.
+ATHB_HD void prim_right_col(const PrimEig& E, int n, double r[7]) {
+  switch (n) {
+  case 0: r[0] = E.R00; r[1] = E.R10;  r[2] = E.R20;  r[3] = E.R30;  r[4] = E.R40; r[5] = E.R50; r[6] = E.R60; break;
+  case 1: r[0] = 0.0;   r[1] = 0.0;    r[2] = E.R21;  r[3] = E.R31;  r[4] = 0.0;   r[5] = E.R51; r[6] = E.R61; break;
+  case 2: r[0] = E.R02; r[1] = E.R12;  r[2] = E.R22;  r[3] = E.R32;  r[4] = E.R42; r[5] = E.R52; r[6] = E.R62; break;
+  case 3: r[0] = 1.0;   r[1] = 0.0;    r[2] = 0.0;    r[3] = 0.0;    r[4] = 0.0;   r[5] = 0.0;   r[6] = 0.0;   break;
+  case 4: r[0] = E.R02; r[1] = -E.R12; r[2] = -E.R22; r[3] = -E.R32; r[4] = E.R42; r[5] = E.R52; r[6] = E.R62; break;
+  case 5: r[0] = 0.0;   r[1] = 0.0;    r[2] = -E.R21; r[3] = -E.R31; r[4] = 0.0;   r[5] = E.R51; r[6] = E.R61; break;
+  default: r[0] = E.R00; r[1] = -E.R10; r[2] = -E.R20; r[3] = -E.R30; r[4] = E.R40; r[5] = E.R50; r[6] = E.R60; break;
+  }
+}
+
+// Structural non-zero masks of the primitive eigenmatrices (bit m of row n).
+// Used to skip exact-zero products; constant-folded after unrolling.
+ATHB_HD int prim_left_mask(int n) {
+  return n == 3 ? 0x11 : (n == 1 || n == 5) ? 0x6C : 0x7E;
+}
+ATHB_HD int prim_right_mask(int n) {  // column n
+  return n == 3 ? 0x01 : (n == 1 || n == 5) ? 0x6C : 0x7F;
+}
+
+// ---------------------------------------------------------------------------
+// Characteristic PLM for one cell (src/lr_states_plm.c:95-233).
+//   wm, w0, wp : primitive states of cells i-1, i, i+1
+//   bxc        : cell-centred normal field of cell i
+// Returns wl_next = W_L at face i+1/2 (reference Wl[i+1]) and
+//         wr_this = W_R at face i-1/2 (reference Wr[i]).
+// ---------------------------------------------------------------------------
+ATHB_HD void plm_cell(const Prim1& wm, const Prim1& w0, const Prim1& wp, double bxc,
+                      double dtodx, const Eos& eos, Prim1& wl_next, Prim1& wr_this) {
+  PrimEig E;
+  esys_prim(w0.d, w0.vx, w0.p, bxc, w0.by, w0.bz, eos, E);
+
+  const double Wm[7] = {wm.d, wm.vx, wm.vy, wm.vz, wm.p, wm.by, wm.bz};
+  const double W0[7] = {w0.d, w0.vx, w0.vy, w0.vz, w0.p, w0.by, w0.bz};
+  const double Wp[7] = {wp.d, wp.vx, wp.vy, wp.vz, wp.p, wp.by, wp.bz};
+
+  // Step 2: centred, left, right and van Leer differences.
+  double dWc[7], dWl[7], dWr[7], dWg[7];
+#pragma unroll
+  for (int n = 0; n < 7; n++) {
+    dWc[n] = Wp[n] - Wm[n];
+    dWl[n] = W0[n] - Wm[n];
+    dWr[n] = Wp[n] - W0[n];
+    if (dWl[n] * dWr[n] > 0.0) dWg[n] = 2.0 * dWl[n] * dWr[n] / (dWl[n] + dWr[n]);
+    else dWg[n] = 0.0;
+  }
+
+  // Step 3: characteristic projections.
+  double dac[7], dal[7], dar[7], dag[7];
+  prim_project(E, dWc, dac);
+  prim_project(E, dWl, dal);
+  prim_project(E, dWr, dar);
+  prim_project(E, dWg, dag);
+
+  // Step 4: monotonicity constraints.
+  double da[7];
+#pragma unroll
+  for (int n = 0; n < 7; n++) {
+    da[n] = 0.0;
+    if (dal[n] * dar[n] > 0.0) {
+      const double lim_slope1 = rmin(fabs(dal[n]), fabs(dar[n]));
+      const double lim_slope2 = rmin(0.5 * fabs(dac[n]), fabs(dag[n]));
+      da[n] = rsign(dac[n]) * rmin(2.0 * lim_slope1, lim_slope2);
+    }
+  }
+
+  // Step 5: back to primitive slopes, dWm[n] = sum_m da[m]*R[n][m].
+  double dWm[7];
+  dWm[0] = da[0] * E.R00 + da[2] * E.R02 + da[3] + da[4] * E.R02 + da[6] * E.R00;
+  dWm[1] = da[0] * E.R10 + da[2] * E.R12 + da[4] * -E.R12 + da[6] * -E.R10;
+  dWm[2] = da[0] * E.R20 + da[1] * E.R21 + da[2] * E.R22 + da[4] * -E.R22 + da[5] * -E.R21 + da[6] * -E.R20;
+  dWm[3] = da[0] * E.R30 + da[1] * E.R31 + da[2] * E.R32 + da[4] * -E.R32 + da[5] * -E.R31 + da[6] * -E.R30;
+  dWm[4] = da[0] * E.R40 + da[2] * E.R42 + da[4] * E.R42 + da[6] * E.R40;
+  dWm[5] = da[0] * E.R50 + da[1] * E.R51 + da[2] * E.R52 + da[4] * E.R52 + da[5] * E.R51 + da[6] * E.R50;
+  dWm[6] = da[0] * E.R60 + da[1] * E.R61 + da[2] * E.R62 + da[4] * E.R62 + da[5] * E.R61 + da[6] * E.R60;
+
+  // Step 7: L/R values, bounded by the neighbouring cell centres.
+  double Wlv[7], Wrv[7], dW[7];
+#pragma unroll
+  for (int n = 0; n < 7; n++) {
+    double l = W0[n] - 0.5 * dWm[n];
+    double r = W0[n] + 0.5 * dWm[n];
+    l = rmax(rmin(W0[n], Wm[n]), l);
+    l = rmin(rmax(W0[n], Wm[n]), l);
+    r = rmax(rmin(W0[n], Wp[n]), r);
+    r = rmin(rmax(W0[n], Wp[n]), r);
+    Wlv[n] = l;
+    Wrv[n] = r;
+    dW[n] = r - l;
+  }
+
+  // Step 8: integrate over the domain of dependence of the extreme waves.
+  double pWl[7], pWr[7];
+  {
+    const double qx = 0.5 * rmax(E.ev[6], 0.0) * dtodx;
+#pragma unroll
+    for (int n = 0; n < 7; n++) pWl[n] = Wrv[n] - qx * dW[n];
+    const double qy = -0.5 * rmin(E.ev[0], 0.0) * dtodx;
+#pragma unroll
+    for (int n = 0; n < 7; n++) pWr[n] = Wlv[n] + qy * dW[n];
+  }
+
+  // Step 9: subtract the waves that do not reach the interface.  Wave 6 in the
+  // first loop and wave 0's first part in the second contribute (ev-ev)=0
+  // multiples of exact-zero size and are skipped.
+#pragma unroll
+  for (int n = 0; n < 6; n++) {
+    if (E.ev[n] > 0.) {
+      double l[7], r[7];
+      prim_left_row(E, n, l);
+      const double dev = E.ev[6] - E.ev[n];
+      double qa = 0.0;
+      bool first = true;
+#pragma unroll
+      for (int m = 0; m < 7; m++) {
+        if (!((prim_left_mask(n) >> m) & 1)) continue;
+        const double t = l[m] * 0.5 * dtodx * dev * dW[m];
+        qa = first ? t : qa + t;
+        first = false;
+      }
+      prim_right_col(E, n, r);
+#pragma unroll
+      for (int m = 0; m < 7; m++)
+        if ((prim_right_mask(n) >> m) & 1) pWl[m] += qa * r[m];
+    }
+  }
+#pragma unroll
+  for (int n = 0; n < 7; n++) {
+    if (E.ev[n] < 0.) {
+      double l[7], r[7], h[7];
+      prim_left_row(E, n, l);
+      prim_right_col(E, n, r);
+#pragma unroll
+      for (int m = 0; m < 7; m++) h[m] = l[m] * 0.5 * dtodx;
+      if (n != 0) {
+        const double dev = E.ev[0] - E.ev[n];
+        double qa = 0.0;
+        bool first = true;
+#pragma unroll
+        for (int m = 0; m < 7; m++) {
+          if (!((prim_left_mask(n) >> m) & 1)) continue;
+          const double t = h[m] * dev * dW[m];
+          qa = first ? t : qa + t;
+          first = false;
+        }
+#pragma unroll
+        for (int m = 0; m < 7; m++)
+          if ((prim_right_mask(n) >> m) & 1) pWr[m] += qa * r[m];
+      }
+      {
+        const double dev = E.ev[n] - E.ev[6];
+        double qa = 0.0;
+        bool first = true;
+#pragma unroll
+        for (int m = 0; m < 7; m++) {
+          if (!((prim_left_mask(n) >> m) & 1)) continue;
+          const double t = h[m] * dev * dW[m];
+          qa = first ? t : qa + t;
+          first = false;
+        }
+#pragma unroll
+        for (int m = 0; m < 7; m++)
+          if ((prim_right_mask(n) >> m) & 1) pWl[m] -= qa * r[m];
+      }
+    }
+  }
+
+  wl_next.d = pWl[0]; wl_next.vx = pWl[1]; wl_next.vy = pWl[2]; wl_next.vz = pWl[3];
+  wl_next.p = pWl[4]; wl_next.by = pWl[5]; wl_next.bz = pWl[6];
+  wr_this.d = pWr[0]; wr_this.vx = pWr[1]; wr_this.vy = pWr[2]; wr_this.vz = pWr[3];
+  wr_this.p = pWr[4]; wr_this.by = pWr[5]; wr_this.bz = pWr[6];
+}
+
+// ---------------------------------------------------------------------------
+// Roe-averaged state shared by the Roe and HLLE solvers
+// (src/flux_roe.c:91-114, src/flux_hlle.c:87-110).
+// ---------------------------------------------------------------------------
+struct RoeAvg {
+  double sqrtdl, sqrtdr, isdlpdr, droe, v1, v2, v3, b2, b3, x, y, pbl, pbr, h;
+};
+
+ATHB_HD RoeAvg roe_average(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const Prim1& Wr,
+                           double Bxi) {
+  RoeAvg r;
+  r.sqrtdl = sqrt(Wl.d);
+  r.sqrtdr = sqrt(Wr.d);
+  r.isdlpdr = 1.0 / (r.sqrtdl + r.sqrtdr);
+  r.droe = r.sqrtdl * r.sqrtdr;
+  r.v1 = (r.sqrtdl * Wl.vx + r.sqrtdr * Wr.vx) * r.isdlpdr;
+  r.v2 = (r.sqrtdl * Wl.vy + r.sqrtdr * Wr.vy) * r.isdlpdr;
+  r.v3 = (r.sqrtdl * Wl.vz + r.sqrtdr * Wr.vz) * r.isdlpdr;
+  r.b2 = (r.sqrtdr * Wl.by + r.sqrtdl * Wr.by) * r.isdlpdr;
+  r.b3 = (r.sqrtdr * Wl.bz + r.sqrtdl * Wr.bz) * r.isdlpdr;
+  const double dby = Wl.by - Wr.by, dbz = Wl.bz - Wr.bz, ss = r.sqrtdl + r.sqrtdr;
+  r.x = 0.5 * (dby * dby + dbz * dbz) / (ss * ss);
+  r.y = 0.5 * (Wl.d + Wr.d) / r.droe;
+  r.pbl = 0.5 * (Bxi * Bxi + Wl.by * Wl.by + Wl.bz * Wl.bz);
+  r.pbr = 0.5 * (Bxi * Bxi + Wr.by * Wr.by + Wr.bz * Wr.bz);
+  r.h = ((Ul.e + Wl.p + r.pbl) / r.sqrtdl + (Ur.e + Wr.p + r.pbr) / r.sqrtdr) * r.isdlpdr;
+  return r;
+}
+
+// Roe-matrix wave speeds (src/esystem_roe.c:68-87,136-144).
+struct RoeSpeeds {
+  double di, vsq, btsq, bt_starsq, vaxsq, hp, twid_asq, cfsq, cf, cssq, cs, vax, gfac;
+};
+
+ATHB_HD RoeSpeeds roe_speeds(const RoeAvg& r, double b1, const Eos& eos) {
+  RoeSpeeds s;
+  s.di = 1.0 / r.droe;
+  s.vsq = r.v1 * r.v1 + r.v2 * r.v2 + r.v3 * r.v3;
+  s.btsq = r.b2 * r.b2 + r.b3 * r.b3;
+  s.gfac = eos.gamma_1 - eos.gamma_2 * r.y;
+  s.bt_starsq = s.gfac * s.btsq;
+  s.vaxsq = b1 * b1 * s.di;
+  s.hp = r.h - (s.vaxsq + s.btsq * s.di);
+  s.twid_asq = rmax((eos.gamma_1 * (s.hp - 0.5 * s.vsq) - eos.gamma_2 * r.x), kTiny);
+  const double ct2 = s.bt_starsq * s.di;
+  const double tsum = s.vaxsq + ct2 + s.twid_asq;
+  const double tdif = s.vaxsq + ct2 - s.twid_asq;
+  const double cf2_cs2 = sqrt(tdif * tdif + 4.0 * s.twid_asq * ct2);
+  s.cfsq = 0.5 * (tsum + cf2_cs2);
+  s.cf = sqrt(s.cfsq);
+  s.cssq = s.twid_asq * s.vaxsq / s.cfsq;
+  s.cs = sqrt(s.cssq);
+  s.vax = sqrt(s.vaxsq);
+  return s;
+}
+
+// Roe eigenvectors (src/esystem_roe.c:91-291) as distinct entries.
+//   R rows 0,1 have zeros in columns 1 and 5; rows 5,6 have a zero in column 3;
+//   R45=-R41, R54=R52, R55=R51, R56=R50 (row 6 likewise).
+//   L rows 1 and 5 have zeros in columns 1 and 4; L5 = (-L10,.,-L12,-L13,.,L15,L16);
+//   L45=L25, L46=L26, L65=L05, L66=L06.
+struct RoeVec {
+  double af, as;  // alpha_f, alpha_s before normalisation (R row 0)
+  double R10, R12, R13, R14, R16;
+  double R20, R21, R22, R23, R24, R25, R26;
+  double R30, R31, R32, R33, R34, R35, R36;
+  double R40, R41, R42, R43, R44, R46;
+  double R50, R51, R52, R60, R61, R62;
+  double L00, L01, L02, L03, L04, L05, L06;
+  double L10, L12, L13, L15, L16;
+  double L20, L21, L22, L23, L24, L25, L26;
+  double L30, L31, L32, L33, L34, L35, L36;
+  double L40, L41, L42, L43;
+  double L60, L61, L62, L63;
+};
+
+ATHB_HD void roe_vectors(const RoeAvg& r, const RoeSpeeds& s, double b1, const Eos& eos,
+                         const double ev[7], RoeVec& V) {
+  const double v1 = r.v1, v2 = r.v2, v3 = r.v3, b2 = r.b2, b3 = r.b3, d = r.droe;
+  const double bt = sqrt(s.btsq);
+  const double bt_star = sqrt(s.bt_starsq);
+  double bet2, bet3;
+  if (bt == 0.0) { bet2 = 1.0; bet3 = 0.0; } else { bet2 = b2 / bt; bet3 = b3 / bt; }
+  const double sg = sqrt(s.gfac);
+  const double bet2_star = bet2 / sg;
+  const double bet3_star = bet3 / sg;
+  const double bet_starsq = bet2_star * bet2_star + bet3_star * bet3_star;
+  const double vbet = v2 * bet2_star + v3 * bet3_star;
+
+  double alpha_f, alpha_s;
+  if ((s.cfsq - s.cssq) == 0.0) { alpha_f = 1.0; alpha_s = 0.0; }
+  else if ((s.twid_asq - s.cssq) <= 0.0) { alpha_f = 0.0; alpha_s = 1.0; }
+  else if ((s.cfsq - s.twid_asq) <= 0.0) { alpha_f = 1.0; alpha_s = 0.0; }
+  else {
+    alpha_f = sqrt((s.twid_asq - s.cssq) / (s.cfsq - s.cssq));
+    alpha_s = sqrt((s.cfsq - s.twid_asq) / (s.cfsq - s.cssq));
+  }
+
+  const double sqrtd = sqrt(d);
+  const double isqrtd = 1.0 / sqrtd;
+  const double sgn = rsign(b1);
+  const double twid_a = sqrt(s.twid_asq);
+  double qf = s.cf * alpha_f * sgn;
+  double qs = s.cs * alpha_s * sgn;
+  const double af_prime = twid_a * alpha_f * isqrtd;
+  const double as_prime = twid_a * alpha_s * isqrtd;
+  const double afpbb = af_prime * bt_star * bet_starsq;
+  const double aspbb = as_prime * bt_star * bet_starsq;
+  const double hp = s.hp, cf = s.cf, cs = s.cs, vsq = s.vsq;
+
+  V.af = alpha_f; V.as = alpha_s;
+  V.R10 = alpha_f * ev[0]; V.R12 = alpha_s * ev[2]; V.R13 = v1; V.R14 = alpha_s * ev[4]; V.R16 = alpha_f * ev[6];
+  {
+    const double qa = alpha_f * v2, qb = alpha_s * v2, qc = qs * bet2_star, qd = qf * bet2_star;
+    V.R20 = qa + qc; V.R21 = -bet3; V.R22 = qb - qd; V.R23 = v2; V.R24 = qb + qd; V.R25 = bet3; V.R26 = qa - qc;
+  }
+  {
+    const double qa = alpha_f * v3, qb = alpha_s * v3, qc = qs * bet3_star, qd = qf * bet3_star;
+    V.R30 = qa + qc; V.R31 = bet2; V.R32 = qb - qd; V.R33 = v3; V.R34 = qb + qd; V.R35 = -bet2; V.R36 = qa - qc;
+  }
+  V.R40 = alpha_f * (hp - v1 * cf) + qs * vbet + aspbb;
+  V.R41 = -(v2 * bet3 - v3 * bet2);
+  V.R42 = alpha_s * (hp - v1 * cs) - qf * vbet - afpbb;
+  V.R43 = 0.5 * vsq + eos.gamma_2 * r.x / eos.gamma_1;
+  V.R44 = alpha_s * (hp + v1 * cs) + qf * vbet - afpbb;
+  V.R46 = alpha_f * (hp + v1 * cf) - qs * vbet + aspbb;
+  V.R50 = as_prime * bet2_star; V.R51 = -bet3 * sgn * isqrtd; V.R52 = -af_prime * bet2_star;
+  V.R60 = as_prime * bet3_star; V.R61 = bet2 * sgn * isqrtd;  V.R62 = -af_prime * bet3_star;
+
+  double norm = 0.5 / s.twid_asq;
+  const double cff = norm * alpha_f * cf;
+  const double css = norm * alpha_s * cs;
+  qf *= norm;
+  qs *= norm;
+  const double af = norm * af_prime * d;
+  const double as = norm * as_prime * d;
+  const double afpb = norm * af_prime * bt_star;
+  const double aspb = norm * as_prime * bt_star;
+
+  norm *= eos.gamma_1;
+  alpha_f *= norm;
+  alpha_s *= norm;
+  const double q2_star = bet2_star / bet_starsq;
+  const double q3_star = bet3_star / bet_starsq;
+  const double vqstr = (v2 * q2_star + v3 * q3_star);
+  norm *= 2.0;
+
+  V.L00 = alpha_f * (vsq - hp) + cff * (cf + v1) - qs * vqstr - aspb;
+  V.L01 = -alpha_f * v1 - cff;
+  V.L02 = -alpha_f * v2 + qs * q2_star;
+  V.L03 = -alpha_f * v3 + qs * q3_star;
+  V.L04 = alpha_f;
+  V.L05 = as * q2_star - alpha_f * b2;
+  V.L06 = as * q3_star - alpha_f * b3;
+
+  V.L10 = 0.5 * (v2 * bet3 - v3 * bet2);
+  V.L12 = -0.5 * bet3;
+  V.L13 = 0.5 * bet2;
+  V.L15 = -0.5 * sqrtd * bet3 * sgn;
+  V.L16 = 0.5 * sqrtd * bet2 * sgn;
+
+  V.L20 = alpha_s * (vsq - hp) + css * (cs + v1) + qf * vqstr + afpb;
+  V.L21 = -alpha_s * v1 - css;
+  V.L22 = -alpha_s * v2 - qf * q2_star;
+  V.L23 = -alpha_s * v3 - qf * q3_star;
+  V.L24 = alpha_s;
+  V.L25 = -af * q2_star - alpha_s * b2;
+  V.L26 = -af * q3_star - alpha_s * b3;
+
+  V.L30 = 1.0 - norm * (0.5 * vsq - eos.gamma_2 * r.x / eos.gamma_1);
+  V.L31 = norm * v1;
+  V.L32 = norm * v2;
+  V.L33 = norm * v3;
+  V.L34 = -norm;
+  V.L35 = norm * b2;
+  V.L36 = norm * b3;
+
+  V.L40 = alpha_s * (vsq - hp) + css * (cs - v1) - qf * vqstr + afpb;
+  V.L41 = -alpha_s * v1 + css;
+  V.L42 = -alpha_s * v2 + qf * q2_star;
+  V.L43 = -alpha_s * v3 + qf * q3_star;
+
+  V.L60 = alpha_f * (vsq - hp) + cff * (cf - v1) + qs * vqstr - aspb;
+  V.L61 = -alpha_f * v1 + cff;
+  V.L62 = -alpha_f * v2 - qs * q2_star;
+  V.L63 = -alpha_f * v3 - qs * q3_star;
+}
+
+// Column n of the Roe right-eigenmatrix (the n-th right eigenvector).
+ATHB_HD void roe_right_col(const RoeVec& V, int n, double c[7]) {
+  switch (n) {
+  case 0: c[0] = V.af; c[1] = V.R10; c[2] = V.R20; c[3] = V.R30; c[4] = V.R40; c[5] = V.R50; c[6] = V.R60; break;
+  case 1: c[0] = 0.0;  c[1] = 0.0;   c[2] = V.R21; c[3] = V.R31; c[4] = V.R41; c[5] = V.R51; c[6] = V.R61; break;
+  case 2: c[0] = V.as; c[1] = V.R12; c[2] = V.R22; c[3] = V.R32; c[4] = V.R42; c[5] = V.R52; c[6] = V.R62; break;
+  case 3: c[0] = 1.0;  c[1] = V.R13; c[2] = V.R23; c[3] = V.R33; c[4] = V.R43; c[5] = 0.0;   c[6] = 0.0;   break;
+  case 4: c[0] = V.as; c[1] = V.R14; c[2] = V.R24; c[3] = V.R34; c[4] = V.R44; c[5] = V.R52; c[6] = V.R62; break;
+  case 5: c[0] = 0.0;  c[1] = 0.0;   c[2] = V.R25; c[3] = V.R35; c[4] = -V.R41; c[5] = V.R51; c[6] = V.R61; break;
+  default: c[0] = V.af; c[1] = V.R16; c[2] = V.R26; c[3] = V.R36; c[4] = V.R46; c[5] = V.R50; c[6] = V.R60; break;
+  }
+}
+ATHB_HD int roe_right_mask(int n) {  // structural non-zeros of column n
+  return (n == 1 || n == 5) ? 0x7C : (n == 3) ? 0x1F : 0x7F;
+}
+
+// a = L * dU (src/flux_roe.c:200-204), terms in column order, zeros skipped.
+ATHB_HD void roe_project(const RoeVec& V, const double u[7], double a[7]) {
+  const double l04 = V.L04 * u[4], l05 = V.L05 * u[5], l06 = V.L06 * u[6];
+  a[0] = V.L00 * u[0] + V.L01 * u[1] + V.L02 * u[2] + V.L03 * u[3] + l04 + l05 + l06;
+  const double p10 = V.L10 * u[0], p12 = V.L12 * u[2], p13 = V.L13 * u[3], p15 = V.L15 * u[5], p16 = V.L16 * u[6];
+  a[1] = p10 + p12 + p13 + p15 + p16;
+  a[5] = -p10 - p12 - p13 + p15 + p16;
+  const double l24 = V.L24 * u[4], l25 = V.L25 * u[5], l26 = V.L26 * u[6];
+  a[2] = V.L20 * u[0] + V.L21 * u[1] + V.L22 * u[2] + V.L23 * u[3] + l24 + l25 + l26;
+  a[3] = V.L30 * u[0] + V.L31 * u[1] + V.L32 * u[2] + V.L33 * u[3] + V.L34 * u[4] + V.L35 * u[5] + V.L36 * u[6];
+  a[4] = V.L40 * u[0] + V.L41 * u[1] + V.L42 * u[2] + V.L43 * u[3] + l24 + l25 + l26;
+  a[6] = V.L60 * u[0] + V.L61 * u[1] + V.L62 * u[2] + V.L63 * u[3] + l04 + l05 + l06;
+}
+
+// Physical flux of one side (src/flux_roe.c:136-172).
+ATHB_HD Cons1 side_flux(const Cons1& U, const Prim1& W, double Bxi, double pb) {
+  Cons1 F;
+  F.d = U.mx;
+  F.mx = U.mx * W.vx;
+  F.my = U.mx * W.vy;
+  F.mz = U.mx * W.vz;
+  F.mx += W.p;
+  F.e = (U.e + W.p) * W.vx;
+  F.mx -= 0.5 * (Bxi * Bxi - W.by * W.by - W.bz * W.bz);
+  F.my -= Bxi * W.by;
+  F.mz -= Bxi * W.bz;
+  F.e += (pb * W.vx - Bxi * (Bxi * W.vx + W.by * W.vy + W.bz * W.vz));
+  F.by = W.by * W.vx - Bxi * W.vy;
+  F.bz = W.bz * W.vx - Bxi * W.vz;
+  return F;
+}
+
+// --- src/flux_hlle.c:60-199 ---------------------------------------------------
+ATHB_HD Cons1 flux_hlle(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const Prim1& Wr,
+                        double Bxi, const Eos& eos) {
+  const RoeAvg r = roe_average(Ul, Ur, Wl, Wr, Bxi);
+  const RoeSpeeds s = roe_speeds(r, Bxi, eos);
+  const double ev0 = r.v1 - s.cf, ev6 = r.v1 + s.cf;
+
+  double asq = eos.gamma * Wl.p / Wl.d;
+  double vaxsq = Bxi * Bxi / Wl.d;
+  double ct2 = (Ul.by * Ul.by + Ul.bz * Ul.bz) / Wl.d;
+  double qsq = vaxsq + ct2 + asq;
+  double tmp = vaxsq + ct2 - asq;
+  double cfsq = 0.5 * (qsq + sqrt(tmp * tmp + 4.0 * asq * ct2));
+  const double cfl = sqrt(cfsq);
+
+  asq = eos.gamma * Wr.p / Wr.d;
+  vaxsq = Bxi * Bxi / Wr.d;
+  ct2 = (Ur.by * Ur.by + Ur.bz * Ur.bz) / Wr.d;
+  qsq = vaxsq + ct2 + asq;
+  tmp = vaxsq + ct2 - asq;
+  cfsq = 0.5 * (qsq + sqrt(tmp * tmp + 4.0 * asq * ct2));
+  const double cfr = sqrt(cfsq);
+
+  const double ar = rmax(ev6, (Wr.vx + cfr));
+  const double al = rmin(ev0, (Wl.vx - cfl));
+  const double bp = rmax(ar, 0.0);
+  const double bm = rmin(al, 0.0);
+
+  Cons1 Fl, Fr;
+  Fl.d = Ul.mx - bm * Ul.d;
+  Fr.d = Ur.mx - bp * Ur.d;
+  Fl.mx = Ul.mx * (Wl.vx - bm);
+  Fr.mx = Ur.mx * (Wr.vx - bp);
+  Fl.my = Ul.my * (Wl.vx - bm);
+  Fr.my = Ur.my * (Wr.vx - bp);
+  Fl.mz = Ul.mz * (Wl.vx - bm);
+  Fr.mz = Ur.mz * (Wr.vx - bp);
+  Fl.mx += Wl.p;
+  Fr.mx += Wr.p;
+  Fl.e = Ul.e * (Wl.vx - bm) + Wl.p * Wl.vx;
+  Fr.e = Ur.e * (Wr.vx - bp) + Wr.p * Wr.vx;
+  Fl.mx -= 0.5 * (Bxi * Bxi - Wl.by * Wl.by - Wl.bz * Wl.bz);
+  Fr.mx -= 0.5 * (Bxi * Bxi - Wr.by * Wr.by - Wr.bz * Wr.bz);
+  Fl.my -= Bxi * Wl.by;
+  Fr.my -= Bxi * Wr.by;
+  Fl.mz -= Bxi * Wl.bz;
+  Fr.mz -= Bxi * Wr.bz;
+  Fl.e += (r.pbl * Wl.vx - Bxi * (Bxi * Wl.vx + Wl.by * Wl.vy + Wl.bz * Wl.vz));
+  Fr.e += (r.pbr * Wr.vx - Bxi * (Bxi * Wr.vx + Wr.by * Wr.vy + Wr.bz * Wr.vz));
+  Fl.by = Wl.by * (Wl.vx - bm) - Bxi * Wl.vy;
+  Fr.by = Wr.by * (Wr.vx - bp) - Bxi * Wr.vy;
+  Fl.bz = Wl.bz * (Wl.vx - bm) - Bxi * Wl.vz;
+  Fr.bz = Wr.bz * (Wr.vx - bp) - Bxi * Wr.vz;
+
+  const double t = 0.5 * (bp + bm) / (bp - bm);
+  Cons1 F;
+  F.d = 0.5 * (Fl.d + Fr.d) + (Fl.d - Fr.d) * t;
+  F.mx = 0.5 * (Fl.mx + Fr.mx) + (Fl.mx - Fr.mx) * t;
+  F.my = 0.5 * (Fl.my + Fr.my) + (Fl.my - Fr.my) * t;
+  F.mz = 0.5 * (Fl.mz + Fr.mz) + (Fl.mz - Fr.mz) * t;
+  F.e = 0.5 * (Fl.e + Fr.e) + (Fl.e - Fr.e) * t;
+  F.by = 0.5 * (Fl.by + Fr.by) + (Fl.by - Fr.by) * t;
+  F.bz = 0.5 * (Fl.bz + Fr.bz) + (Fl.bz - Fr.bz) * t;
+  return F;
+}
+
+// --- src/flux_roe.c:54-259 ----------------------------------------------------
+ATHB_HD Cons1 flux_roe(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const Prim1& Wr,
+                       double Bxi, const Eos& eos) {
+  const RoeAvg r = roe_average(Ul, Ur, Wl, Wr, Bxi);
+  const RoeSpeeds s = roe_speeds(r, Bxi, eos);
+  double ev[7];
+  ev[0] = r.v1 - s.cf; ev[1] = r.v1 - s.vax; ev[2] = r.v1 - s.cs; ev[3] = r.v1;
+  ev[4] = r.v1 + s.cs; ev[5] = r.v1 + s.vax; ev[6] = r.v1 + s.cf;
+
+  const Cons1 Fl = side_flux(Ul, Wl, Bxi, r.pbl);
+  const Cons1 Fr = side_flux(Ur, Wr, Bxi, r.pbr);
+
+  // Step 5: supersonic faces take the upwind flux.
+  if (ev[0] >= 0.0) return Fl;
+  if (ev[6] <= 0.0) return Fr;
+
+  RoeVec V;
+  roe_vectors(r, s, Bxi, eos, ev, V);
+
+  // Step 6: wave strengths.
+  const double dU[7] = {Ur.d - Ul.d, Ur.mx - Ul.mx, Ur.my - Ul.my, Ur.mz - Ul.mz,
+                        Ur.e - Ul.e, Ur.by - Ul.by, Ur.bz - Ul.bz};
+  double a[7];
+  roe_project(V, dU, a);
+
+  // Step 7: positivity of the intermediate states; HLLE if violated.
+  {
+    double u[7] = {Ul.d, Ul.mx, Ul.my, Ul.mz, Ul.e, Ul.by, Ul.bz};
+    bool hlle = false;
+#pragma unroll
+    for (int n = 0; n < 6; n++) {
+      double c[7];
+      roe_right_col(V, n, c);
+#pragma unroll
+      for (int m = 0; m < 7; m++)
+        if ((roe_right_mask(n) >> m) & 1) u[m] += a[n] * c[m];
+      if (ev[n + 1] > ev[n]) {
+        if (u[0] <= 0.0) { hlle = true; break; }
+        double p_inter = u[4] - 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0];
+        p_inter -= 0.5 * (u[5] * u[5] + u[6] * u[6] + Bxi * Bxi);
+        if (p_inter < 0.0) { hlle = true; break; }
+      }
+    }
+    if (hlle) return flux_hlle(Ul, Ur, Wl, Wr, Bxi, eos);
+  }
+
+  // Step 8: Roe flux.
+  double coeff[7];
+#pragma unroll
+  for (int m = 0; m < 7; m++) coeff[m] = 0.5 * rmax(fabs(ev[m]), 0.0) * a[m];
+  double F[7] = {0.5 * (Fl.d + Fr.d), 0.5 * (Fl.mx + Fr.mx), 0.5 * (Fl.my + Fr.my),
+                 0.5 * (Fl.mz + Fr.mz), 0.5 * (Fl.e + Fr.e), 0.5 * (Fl.by + Fr.by),
+                 0.5 * (Fl.bz + Fr.bz)};
+#pragma unroll
+  for (int m = 0; m < 7; m++) {
+    double c[7];
+    roe_right_col(V, m, c);
+#pragma unroll
+    for (int n = 0; n < 7; n++)
+      if ((roe_right_mask(m) >> n) & 1) F[n] -= coeff[m] * c[n];
+  }
+  Cons1 out;
+  out.d = F[0]; out.mx = F[1]; out.my = F[2]; out.mz = F[3]; out.e = F[4]; out.by = F[5]; out.bz = F[6];
+  return out;
+}
+
+// Flux selection: the reference always calls flux_roe (src/__integrate_2d__.c:178,
+// 238,444,461); HLLE everywhere is the optional alternative.
+enum FluxKind { kFluxRoe = 0, kFluxHlle = 1 };
+
+template <int FLUX>
+ATHB_HD Cons1 riemann(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const Prim1& Wr,
+                      double Bxi, const Eos& eos) {
+  if (FLUX == kFluxHlle) return flux_hlle(Ul, Ur, Wl, Wr, Bxi, eos);
+  return flux_roe(Ul, Ur, Wl, Wr, Bxi, eos);
+}
+
+}  // namespace athb

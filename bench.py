@@ -1,0 +1,334 @@
+#!/usr/bin/env python
+"""Throughput of the FP64 2D ideal-MHD CTU+CT step on B200, in zone-cycles/s.
+
+Workload: the field-loop advection problem (reference src/field_loop.c) on
+2048 x 2048 cells, [-1,1] x [-0.5,0.5], periodic, v = (2,1), gamma = 5/3, Roe
+fluxes, CFL 0.8.  A "step" is one iteration of the reference main loop
+(src/main.c:229-307): integrate_2d, time += dt, new_dt, set_bvals.  The state
+(372 MB) and the per-step face scratch (1.9 GB) are far larger than the 126 MB
+L2, so every step streams from HBM.
+
+Arms:
+  default            sm_100a kernels, device-resident state, CUDA graph; the
+                     device-timed `value`, the per-kernel roofline, `e2e`
+                     through the reference-named drop-in ABI on pinned host
+                     buffers, and a CPU baseline (the reference's own CPU path)
+  --impl reference   the reference CPU path (oracle/_ref) on all host cores
+
+Under torchrun (N > 1) every rank runs an independent replica of the
+workload (the single-grid step does not shard): weak scaling, max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "zone-cycles/s (FP64 CTU+CT step, bit-exact vs reference)"
+UNIT = "zone-cycles/s"
+
+# Algorithmic FP64 operations (+ - * / sqrt on Real, each counted once) per
+# zone-cycle of the reference's integrate_2d for this workload, split by the
+# kernel that performs them; measured by oracle/opcount.
+OPS_FILE = ROOT / "profiles" / "opcount_field_loop_2048.json"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nx", type=int, default=2048)
+    ap.add_argument("--ny", type=int, default=2048)
+    ap.add_argument("--e2e-steps", type=int, default=8)
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def config_dict(a):
+    return {"workload": f"field_loop {a.nx}x{a.ny}", "problem": "field_loop", "nx1": a.nx, "nx2": a.ny,
+            "flux": "roe", "precision": "fp64", "cfl": 0.8, "l2": "inputs larger than L2 (372 MB state)",
+            "parallelism": "replicas" if a.gpus > 1 else "single"}
+
+
+def write_input(a, d: Path, device: int = 0) -> Path:
+    from athena_cuda_b200 import configs, write_athinput
+    blocks = configs.field_loop(a.nx, a.ny)
+    blocks["job"]["device"] = device
+    return write_athinput(d / "athinput.field_loop", blocks)
+
+
+# ---------------------------------------------------------------------------
+# CPU reference (oracle/_ref)
+# ---------------------------------------------------------------------------
+def ref_exe() -> Path:
+    return ROOT / "oracle" / "_ref" / "athref_field_loop_roe"
+
+
+def run_ref_sample(ath: Path, steps: int, procs: int, workdir: Path, max_seconds: float = 25.0) -> dict:
+    """`procs` concurrent single-threaded reference processes, each running
+    `steps` main-loop iterations (or fewer once its loop has run max_seconds);
+    zone-cycles/s summed over processes (each process times its own main loop,
+    setup excluded)."""
+    exe = ref_exe()
+    ps = [subprocess.Popen([str(exe), "-i", str(ath), "--steps", str(steps), "--bench",
+                            "--max-seconds", str(max_seconds)],
+                           stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, cwd=workdir, text=True)
+          for _ in range(procs)]
+    outs = []
+    for p in ps:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            raise RuntimeError("reference run failed")
+        outs.append(json.loads(out.strip().splitlines()[-1]))
+    total = sum(o["zone_cycles_per_s"] for o in outs)
+    return {"value": total, "per_process": [o["zone_cycles_per_s"] for o in outs],
+            "seconds": max(o["seconds"] for o in outs)}
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def reference_arm(a) -> None:
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    if not ref_exe().exists():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (python oracle/build_ref.py)"}))
+        return
+    cores = max(1, min(os.cpu_count() or 1, 16))
+    with tempfile.TemporaryDirectory() as td:
+        td = Path(td)
+        ath = write_input(a, td)
+        # one bounded sample: every process runs the timed steps (capped at
+        # ~20 s of main loop); the warm-up is the page-in of the first step
+        r = run_ref_sample(ath, max(1, min(a.steps, 3)), cores, td, max_seconds=20.0)
+        value = r["value"]
+    cells = a.nx * a.ny
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * cells * cores / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (field-loop initial condition, src/field_loop.c)",
+        "config": config_dict(a),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"{cores} concurrent single-threaded reference processes (-O2 "
+                                   f"-ffp-contract=off), each up to {max(1, min(a.steps, 3))} main-loop "
+                                   f"iterations (<= 20 s) of the {a.nx}x{a.ny} field loop; {cpu_model()}"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device, self.proc, self.path = device, None, None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.path = Path(tempfile.mkstemp(suffix=".csv")[1])
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict | None:
+        if not self.path or not self.path.exists():
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        self.path.unlink(missing_ok=True)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def ours(a) -> None:
+    import ctypes as C
+
+    import torch
+
+    import athena_cuda_b200 as ab
+    from athena_cuda_b200 import Grid, lib
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local))
+    L = lib()
+    L.athb_profile_steps.restype, L.athb_profile_steps.argtypes = C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
+    L.athb_fp64_peak.restype, L.athb_fp64_peak.argtypes = C.c_int, [C.c_int, C.POINTER(C.c_double)]
+
+    td = Path(tempfile.mkdtemp())
+    ath = write_input(a, td, local)
+    g = Grid.from_athinput(ath, "field_loop")
+    g.run(a.warmup)
+    st0 = g.status()
+    stream = torch.cuda.ExternalStream(g.stream, device=torch.device("cuda", local))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        g.run_async(a.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    st1 = g.status()
+    assert st1["nstep"] - st0["nstep"] == a.steps and not st1["done"], "timed steps did not all run"
+    if ws > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    cells = a.nx * a.ny
+    ms_step = ms / a.steps
+    value = ws * cells / (ms_step * 1e-3)
+
+    # per-kernel event timing (same stream, outside the graph)
+    kms = (C.c_double * 7)()
+    rc = L.athb_profile_steps(g._h, 10, kms)
+    if rc:
+        raise RuntimeError(L.athb_last_error().decode())
+    names = ["predict", "emf_half", "correct", "emf_full", "update_cfl", "finalize", "ghost"]
+    kernel_ms = dict(zip(names, list(kms)))
+    peak = C.c_double()
+    rc = L.athb_fp64_peak(local, C.byref(peak))
+    if rc:
+        raise RuntimeError(L.athb_last_error().decode())
+    roofline = None
+    if OPS_FILE.exists():
+        ops = json.loads(OPS_FILE.read_text())
+        top = max(("predict", "correct"), key=lambda k: kernel_ms[k])
+        per_launch = ops["per_kernel_ops"][top]  # ops per launch at this size
+        achieved = per_launch / (kernel_ms[top] * 1e-3)
+        step_ops = ops["ops_per_zone_cycle"] * cells
+        roofline = {"bound": "fp64", "kernel": f"k_{top}", "achieved": achieved / 1e12,
+                    "peak": peak.value / 1e12, "unit": "TFLOP/s", "frac": achieved / peak.value,
+                    "peak_kind": "measured FP64 add/mul issue rate (athb_fp64_peak, no FMA)",
+                    "traffic": ops.get("traffic", {}).get(top),
+                    "step_achieved": step_ops / (ms_step * 1e-3) / 1e12,
+                    "step_frac": step_ops / (ms_step * 1e-3) / peak.value,
+                    "kernel_ms": kernel_ms}
+    g.close()
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (field-loop initial condition, src/field_loop.c)",
+            "config": config_dict(a), "gpu_launches": 7 * a.steps, "roofline": roofline,
+            "clocks": clk.summary()}
+
+    if rank == 0 and not a.no_e2e:
+        line["e2e"] = e2e(a, ath)
+    if rank == 0 and ws == 1 and not a.no_cpu and ref_exe().exists():
+        r = run_ref_sample(ath, a.cpu_steps, 1, td)
+        line["cpu_baseline"] = {"value": r["value"], "unit": UNIT, "cores": 1, "kind": "reference",
+                                "sample": f"{a.cpu_steps} main-loop iterations of the {a.nx}x{a.ny} field loop, "
+                                          f"1 reference process (-O2 -ffp-contract=off), {cpu_model()}"}
+    if rank == 0:
+        print(json.dumps(line))
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def e2e(a, ath: Path) -> dict:
+    """The same metric through the reference-named drop-in ABI: the host Grid
+    (pinned) is the state; every step copies it to the GPU and the result back."""
+    from athena_cuda_b200 import Params, configs, problem_state
+    from athena_cuda_b200.dropin import DropInLoop, HostGrid
+
+    p = Params(ath)
+    cfg = p.config()
+    planes = problem_state("field_loop", p)
+    dx1, dx2 = (cfg.x1max - cfg.x1min) / cfg.nx1, (cfg.x2max - cfg.x2min) / cfg.nx2
+    hg = HostGrid(planes, dx1, dx2, cfg.x1min, cfg.x2min)
+    loop = DropInLoop(hg, configs.GAMMA, cfg.cour_no, bc=(4, 4, 4, 4))
+    loop.steps(2)  # warm-up
+    h0, d0 = loop.bytes_moved()
+    t0 = time.perf_counter()
+    n = loop.steps(a.e2e_steps)
+    dt = time.perf_counter() - t0
+    h1, d1 = loop.bytes_moved()
+    loop.close()
+    hg.close()
+    return {"value": a.nx * a.ny * n / dt, "unit": UNIT, "h2d_bytes_per_step": (h1 - h0) // n,
+            "d2h_bytes_per_step": (d1 - d0) // n, "steps": n,
+            "path": "integrate_2d + new_dt + set_bvals drop-in calls on a pinned host Grid"}
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        reference_arm(a)
+    else:
+        ours(a)
+
+
+if __name__ == "__main__":
+    main()

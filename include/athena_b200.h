@@ -1,0 +1,204 @@
+/*
+ * athena_b200.h -- C ABI of libathena_b200.so, a B200 (sm_100a) implementation
+ * of the 2D adiabatic ideal-MHD CTU+CT step of Athena 3.1 as cut down in
+ * awasiljew/athena-cuda.
+ *
+ * Two layers:
+ *
+ *  1. Drop-in entry points with the reference's names, signatures and Grid
+ *     layout, so a program built against the reference CPU path links against
+ *     this library instead of src/__integrate_2d__.c, src/lr_states_plm.c,
+ *     src/set_bvals.c and src/new_dt.c.  They work on HOST Grid buffers: each
+ *     call copies what it needs to the GPU and the result back.
+ *
+ *  2. The device-resident athb_* API: the grid lives in HBM between calls and
+ *     a whole loop of steps runs without host round trips (CUDA graph).
+ *
+ * Every athb_* function returns ATHB_OK (0) or an ATHB_ERR_* code and never
+ * exits the process; athb_last_error() gives the message of the calling
+ * thread's last failure.  The drop-in functions keep the reference's
+ * convention: a fatal error prints a message and exits (src/utils.c:111-127).
+ *
+ * Threading: one context is used by one host thread at a time.
+ */
+#ifndef ATHENA_B200_H
+#define ATHENA_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Reference data layout (src/athena.h:43-52 Gas, src/athena.h:106-120 Grid). */
+/* Field order and types are identical, so a reference Grid* can be passed.   */
+/* ------------------------------------------------------------------------ */
+typedef struct athb_Gas {
+  double d, M1, M2, M3, E, B1c, B2c, B3c;
+} athb_Gas;
+
+typedef struct athb_Grid {
+  athb_Gas **U;                 /* [Nx2+8][Nx1+8] cell-centred conserved   */
+  double **B1i, **B2i, **B3i;   /* [Nx2+8][Nx1+8] face-centred fields      */
+  double x1_0, x2_0;
+  double dx1, dx2;
+  double dt, time;
+  int nstep;
+  int Nx1, Nx2;
+  int is, ie, js, je;
+  int idisp, jdisp;
+  char *outfilename;
+} athb_Grid;
+
+typedef void (*athb_VBCFun_t)(athb_Grid *pG, int var_flag);
+
+/* Reference globals (src/globals.h:18-20).  Defined weakly by the library so
+ * a host program that defines them (src/main.c with MAIN_C) supplies them. */
+extern double Gamma, Gamma_1, Gamma_2, CourNo;
+
+/* ---- drop-in entry points (reference names) ----------------------------- */
+/* replaces src/__integrate_2d__.c:573 integrate_init_2d(int nx1, int nx2)   */
+void integrate_init_2d(int nx1, int nx2);
+/* replaces src/__integrate_2d__.c:543 integrate_destruct_2d(void)           */
+void integrate_destruct_2d(void);
+/* replaces src/__integrate_2d__.c:100 integrate_2d(Grid *pG): one CTU+CT
+ * step with pG->dt; writes U (interior), B1i (interior + column ie+1),
+ * B2i (interior + row je+1) and B3i (interior), exactly as the reference.   */
+void integrate_2d(athb_Grid *pG);
+/* replaces src/lr_states_plm.c:253 / :270 (no state needed on the GPU)      */
+void lr_states_init(int nx1, int nx2);
+void lr_states_destruct(void);
+/* replaces src/set_bvals.c:152 set_bvals_init(Grid*): reads grid/ibc_x1,
+ * obc_x1, ibc_x2, obc_x2 through the host program's par_geti() (src/par.c)
+ * unless athb_dropin_set_bc() set them first.                               */
+void set_bvals_init(athb_Grid *pG);
+/* replaces src/set_bvals.c:114 set_bvals(Grid*, int var_flag)               */
+void set_bvals(athb_Grid *pG, int var_flag);
+/* replaces src/set_bvals.c:269 set_bvals_fun(enum Direction, VBCFun_t):
+ * dir 0..3 = left_x1, right_x1, left_x2, right_x2.  A user function runs on
+ * the host Grid at its place in the x1-then-x2 order.                       */
+void set_bvals_fun(int dir, athb_VBCFun_t prob_bc);
+/* replaces src/new_dt.c:25 new_dt(Grid*): CFL reduction on the GPU, then the
+ * reference dt rule (first step / at most 2x growth) on pG->dt.             */
+void new_dt(athb_Grid *pG);
+
+/* ---- status codes -------------------------------------------------------- */
+#define ATHB_OK 0
+#define ATHB_ERR_ARG 1      /* invalid argument or size                      */
+#define ATHB_ERR_CUDA 2     /* CUDA runtime error (message has the detail)   */
+#define ATHB_ERR_STATE 3    /* device flagged a non-finite / negative 1/dt   */
+#define ATHB_ERR_PARSE 4    /* athinput file or parameter error              */
+#define ATHB_ERR_NOMEM 5    /* allocation failure                            */
+#define ATHB_ERR_NOTFOUND 6 /* unknown problem generator / parameter         */
+
+#define ATHB_FLUX_ROE 0     /* reference default (flux_roe, HLLE fallback)   */
+#define ATHB_FLUX_HLLE 1    /* flux_hlle everywhere                          */
+
+#define ATHB_BC_REFLECT 1   /* src/set_bvals.c:166-181 flag values           */
+#define ATHB_BC_OUTFLOW 2
+#define ATHB_BC_PERIODIC 4
+
+#define ATHB_NPLANES 11     /* d M1 M2 M3 E B1c B2c B3c B1i B2i B3i          */
+
+typedef struct athb_ctx athb_ctx;
+
+typedef struct athb_config {
+  int nx1, nx2;                 /* interior cells, each >= 4                 */
+  double x1min, x1max, x2min, x2max;
+  int bc_ix1, bc_ox1, bc_ix2, bc_ox2;  /* ATHB_BC_*                          */
+  double gamma;                 /* Gamma_1 = gamma-1, Gamma_2 = gamma-2      */
+  double cour_no;               /* CFL number                                */
+  double tlim;                  /* loop ends when time >= tlim               */
+  int nlim;                     /* ... or nstep >= nlim (nlim < 0: no limit) */
+  int flux;                     /* ATHB_FLUX_*                               */
+  int device;                   /* CUDA device ordinal                       */
+} athb_config;
+
+const char *athb_error_string(int code);
+const char *athb_last_error(void);
+
+int athb_create(const athb_config *cfg, athb_ctx **out);
+void athb_destroy(athb_ctx *ctx);
+
+/* Host layout of a state: ATHB_NPLANES planes of (nx2+8) x (nx1+8) doubles,
+ * row-major, ghosts included, plane order d M1 M2 M3 E B1c B2c B3c B1i B2i B3i. */
+int athb_shape(const athb_ctx *ctx, int *sx, int *sy);
+int athb_upload(athb_ctx *ctx, const double *planes, double dt, double time, int nstep);
+int athb_download(athb_ctx *ctx, double *planes, double *dt, double *time, int *nstep);
+
+/* Ghost fill of the resident state (src/set_bvals.c:114).                   */
+int athb_set_bvals(athb_ctx *ctx);
+/* CFL dt of the resident state with the reference rule; stores and returns
+ * it and applies the tlim clamp for the next step (src/main.c:230-232).     */
+int athb_new_dt(athb_ctx *ctx, double *dt);
+/* Run up to nsteps iterations of the reference main loop (clamp, step,
+ * time += dt, new_dt, set_bvals) on the device; stops early at tlim/nlim.   */
+int athb_run(athb_ctx *ctx, int nsteps, int *steps_done);
+int athb_status(athb_ctx *ctx, double *time, double *dt, int *nstep, int *done);
+int athb_synchronize(athb_ctx *ctx);
+/* Launch-only variant of athb_run for timing (no synchronisation).          */
+int athb_run_async(athb_ctx *ctx, int nsteps);
+/* Run nsteps loop iterations with CUDA events between the kernels and return
+ * the mean time per step of each kernel in ms_out[7]: predict, emf (half
+ * step), correct, emf (full step), update (+CFL), finalize, ghost.          */
+int athb_profile_steps(athb_ctx *ctx, int nsteps, double *ms_out);
+/* The CUDA stream the context launches on (as a cudaStream_t).               */
+void *athb_stream(athb_ctx *ctx);
+
+/* Pinned host memory for fast transfers. */
+void *athb_host_alloc(unsigned long long bytes);
+void athb_host_free(void *p);
+
+/* ---- athinput (src/par.c format) and problem generators ---------------- */
+typedef struct athb_params athb_params;
+int athb_params_open(const char *path, athb_params **out);
+/* "block/name=value" overrides of existing keys (src/par.c:170-209)         */
+int athb_params_override(athb_params *p, const char *arg);
+int athb_params_getd(const athb_params *p, const char *block, const char *name, double *v);
+int athb_params_geti(const athb_params *p, const char *block, const char *name, int *v);
+void athb_params_close(athb_params *p);
+/* config from the <grid>, <time> and <problem> blocks */
+int athb_config_from_params(const athb_params *p, athb_config *cfg);
+
+/* Problem generator hook: fill the interior cells and the interior faces
+ * (including B1i column ie+1 and B2i row je+1) of a host state laid out as
+ * in athb_upload.  Built in: "blast" (src/blast.c:25-72), "field_loop"
+ * (src/field_loop.c:40-137), "cpaw2d" (src/cpaw2d.c:56-185).                */
+typedef struct athb_grid_info {
+  int nx1, nx2, sx, sy, is, ie, js, je;
+  double dx1, dx2, x1_0, x2_0;
+  int idisp, jdisp;
+  double gamma, gamma_1, gamma_2;
+} athb_grid_info;
+typedef int (*athb_problem_fn)(const athb_grid_info *g, const athb_params *p,
+                               double *planes, void *user);
+int athb_register_problem(const char *name, athb_problem_fn fn, void *user);
+int athb_grid_info_of(const athb_ctx *ctx, athb_grid_info *g);
+int athb_problem_generate(const char *name, const athb_grid_info *g, const athb_params *p,
+                          double *planes);
+
+/* Parse an athinput file (+ overrides), create the context, run the problem
+ * generator, set_bvals and the first new_dt: the state src/main.c:75-149
+ * holds on entry to its main loop.                                          */
+int athb_create_from_athinput(const char *path, int noverride, const char *const *overrides,
+                              const char *problem, athb_ctx **out);
+
+/* cpaw2d L1 errors against the initial state (src/cpaw2d.c:222-302,
+ * Userwork_after_loop): err[0]=RMS, err[1..8] = d M1 M2 M3 E B1c B2c B3c,
+ * each divided by Nx1*Nx2.  Only for contexts created by cpaw2d.            */
+int athb_cpaw2d_errors(athb_ctx *ctx, double err[9]);
+
+/* Drop-in configuration without the host program's par.c.                  */
+void athb_dropin_set_bc(int ibc_x1, int obc_x1, int ibc_x2, int obc_x2);
+void athb_dropin_set_flux(int flux);
+/* Bytes the drop-in entry points have copied host->device / device->host.  */
+void athb_dropin_bytes(unsigned long long *h2d, unsigned long long *d2h);
+
+/* Measured FP64 issue rate of this GPU: add/mul operations per second from
+ * independent chains of DADD and DMUL (no fused multiply-add, like the step),
+ * timed with CUDA events.  The roofline denominator of the FP64-bound step.  */
+int athb_fp64_peak(int device, double *ops_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ATHENA_B200_H */
