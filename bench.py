@@ -38,16 +38,28 @@ sys.path.insert(0, str(ROOT))
 METRIC = "zone-cycles/s (FP64 CTU+CT step, bit-exact vs reference)"
 UNIT = "zone-cycles/s"
 
-# Algorithmic FP64 operations (+ - * / sqrt on Real, each counted once) per
-# zone-cycle of the reference's integrate_2d for this workload, split by the
-# kernel that performs them; measured by oracle/opcount.
-OPS_FILE = ROOT / "profiles" / "opcount_field_loop_2048.json"
+# Algorithmic FP64 operations per zone-cycle of the reference step on the
+# 2048x2048 field loop (every binary + - * / and sqrt on a Real that the
+# reference performs), split by the kernel that performs them.  Counted by
+# `python oracle/opcount.py --problem field_loop --nx 2048 --ny 2048 --steps 3`
+# (profiles/opcount_field_loop_2048.md).  Per launch = value x nx x ny.
+OPS_PER_ZC = {
+    "predict": 3432.2,     # steps 1a-2e and 3 (PLM, MHD source, Roe, emf3_cc)
+    "emf_half": 18.0,      # step 4 corner EMF + half-step CT
+    "correct": 1378.6,     # steps 5a-8c (transverse terms, emf3_cc n+1/2, Roe)
+    "emf_full": 12.0,      # step 9 corner EMF
+    "update_cfl": 129.0,   # steps 9 CT, 11a, 11b, 13 (52) + new_dt (77)
+}
+OPS_STEP = sum(OPS_PER_ZC.values())
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# dominant kernels from one ncu capture (profiles/), scaled to 2048x2048.
+TRAFFIC: dict = {}
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nx", type=int, default=2048)
@@ -261,20 +273,18 @@ def ours(a) -> None:
     rc = L.athb_fp64_peak(local, C.byref(peak))
     if rc:
         raise RuntimeError(L.athb_last_error().decode())
-    roofline = None
-    if OPS_FILE.exists():
-        ops = json.loads(OPS_FILE.read_text())
-        top = max(("predict", "correct"), key=lambda k: kernel_ms[k])
-        per_launch = ops["per_kernel_ops"][top]  # ops per launch at this size
-        achieved = per_launch / (kernel_ms[top] * 1e-3)
-        step_ops = ops["ops_per_zone_cycle"] * cells
-        roofline = {"bound": "fp64", "kernel": f"k_{top}", "achieved": achieved / 1e12,
-                    "peak": peak.value / 1e12, "unit": "TFLOP/s", "frac": achieved / peak.value,
-                    "peak_kind": "measured FP64 add/mul issue rate (athb_fp64_peak, no FMA)",
-                    "traffic": ops.get("traffic", {}).get(top),
-                    "step_achieved": step_ops / (ms_step * 1e-3) / 1e12,
-                    "step_frac": step_ops / (ms_step * 1e-3) / peak.value,
-                    "kernel_ms": kernel_ms}
+    top = max(("predict", "correct"), key=lambda k: kernel_ms[k])
+    per_launch = OPS_PER_ZC[top] * cells
+    achieved = per_launch / (kernel_ms[top] * 1e-3)
+    step_ops = OPS_STEP * cells
+    roofline = {"bound": "fp64", "kernel": f"k_{top}", "achieved": achieved / 1e12,
+                "peak": peak.value / 1e12, "unit": "TFLOP/s", "frac": achieved / peak.value,
+                "peak_kind": "measured FP64 add/mul issue rate on this GPU (athb_fp64_peak, no FMA)",
+                "algorithmic_ops_per_launch": per_launch,
+                "traffic": TRAFFIC.get(top),
+                "step_achieved": step_ops / (ms_step * 1e-3) / 1e12,
+                "step_frac": step_ops / (ms_step * 1e-3) / peak.value,
+                "kernel_ms": kernel_ms}
     g.close()
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps,
