@@ -83,6 +83,24 @@ def lib() -> C.CDLL:
             "athb_config_from_params": (I, [P, C.POINTER(Config)]),
             "athb_problem_generate": (I, [C.c_char_p, C.POINTER(GridInfo), P, dp]),
             "athb_host_alloc": (P, [C.c_ulonglong]),
+            "athb_params_from_string": (I, [C.c_char_p, C.POINTER(P)]),
+            "athb_batch_create": (I, [I, C.POINTER(Config), C.POINTER(P)]),
+            "athb_batch_destroy": (None, [P]),
+            "athb_batch_upload": (I, [P, I, dp, D, D, I]),
+            "athb_batch_download": (I, [P, I, dp, dp, dp, ip]),
+            "athb_batch_prepare": (I, [P]),
+            "athb_batch_run": (I, [P, I, ip]),
+            "athb_batch_run_async": (I, [P, I]),
+            "athb_batch_synchronize": (I, [P]),
+            "athb_batch_stream": (P, [P]),
+            "athb_batch_set_ly": (I, [P, I, I]),
+            "athb_batch_commit": (I, [P]),
+            "athb_batch_set_grid": (I, [P, I]),
+            "athb_batch_grid": (I, [P]),
+            "athb_profile_steps": (I, [P, I, dp]),
+            "athb_fp64_peak": (I, [I, dp]),
+            "athb_set_ly": (I, [P, I]),
+            "athb_get_ly": (I, [P]),
             "athb_host_free": (None, [P]),
         }
         for name, (res, args) in sig.items():
@@ -104,11 +122,18 @@ def _dp(a: np.ndarray):
 class Params:
     """An athinput parameter file (reference src/par.c format)."""
 
-    def __init__(self, path: str | os.PathLike, overrides: list[str] = ()):
+    def __init__(self, path: str | os.PathLike | None, overrides: list[str] = (), text: str | None = None):
         self._h = C.c_void_p()
-        _check(lib().athb_params_open(str(path).encode(), C.byref(self._h)))
+        if text is not None:
+            _check(lib().athb_params_from_string(text.encode(), C.byref(self._h)))
+        else:
+            _check(lib().athb_params_open(str(path).encode(), C.byref(self._h)))
         for o in overrides:
             _check(lib().athb_params_override(self._h, o.encode()))
+
+    @classmethod
+    def from_blocks(cls, blocks: dict) -> "Params":
+        return cls(None, text=athinput_text(blocks))
 
     def getd(self, block: str, name: str) -> float:
         v = C.c_double()
@@ -223,6 +248,20 @@ class Grid:
     def stream(self) -> int:
         return lib().athb_stream(self._h) or 0
 
+    @property
+    def ly(self) -> int:
+        return lib().athb_get_ly(self._h)
+
+    @ly.setter
+    def ly(self, v: int) -> None:
+        _check(lib().athb_set_ly(self._h, v))
+
+    def profile(self, nsteps: int = 5) -> dict:
+        """Mean ms per step of each kernel (CUDA events between launches)."""
+        ms = (C.c_double * 7)()
+        _check(lib().athb_profile_steps(self._h, nsteps, ms))
+        return dict(zip(("predict", "emf_half", "correct", "emf_full", "update_cfl", "finalize", "ghost"), ms))
+
     def cpaw2d_errors(self) -> np.ndarray:
         err = np.zeros(9)
         _check(lib().athb_cpaw2d_errors(self._h, _dp(err)))
@@ -240,14 +279,95 @@ class Grid:
             pass
 
 
-def write_athinput(path, blocks: dict) -> Path:
-    """Write an athinput file from {block: {name: value}} (reference format)."""
-    path = Path(path)
+def athinput_text(blocks: dict) -> str:
+    """athinput text from {block: {name: value}} (reference format)."""
     lines = []
     for b, kv in blocks.items():
         lines.append(f"<{b}>")
         for k, v in kv.items():
             lines.append(f"{k} = {v!r}" if isinstance(v, float) else f"{k} = {v}")
         lines.append("")
-    path.write_text("\n".join(lines))
+    return "\n".join(lines)
+
+
+def write_athinput(path, blocks: dict) -> Path:
+    """Write an athinput file from {block: {name: value}} (reference format)."""
+    path = Path(path)
+    path.write_text(athinput_text(blocks))
     return path
+
+
+class Batch:
+    """Independent grids advanced together, one persistent launch per step."""
+
+    def __init__(self, cfgs: list[Config]):
+        arr = (Config * len(cfgs))(*cfgs)
+        self._h = C.c_void_p()
+        _check(lib().athb_batch_create(len(cfgs), arr, C.byref(self._h)))
+        self.n = len(cfgs)
+        self.shapes = [(c.nx2 + 2 * NGHOST, c.nx1 + 2 * NGHOST) for c in cfgs]
+
+    @classmethod
+    def from_problems(cls, items: list[tuple[str, dict]]) -> "Batch":
+        """items: (problem name, athinput blocks) per instance; runs each
+        problem generator, set_bvals and the first new_dt."""
+        params = [Params.from_blocks(b) for _, b in items]
+        cfgs = [p.config() for p in params]
+        b = cls(cfgs)
+        for k, ((name, _), p) in enumerate(zip(items, params)):
+            b.upload(k, problem_state(name, p))
+        b.prepare()
+        return b
+
+    def upload(self, k: int, planes: np.ndarray, dt=0.0, time=0.0, nstep=0) -> None:
+        planes = np.ascontiguousarray(planes, dtype=np.float64)
+        assert planes.shape == (NPLANES, *self.shapes[k])
+        _check(lib().athb_batch_upload(self._h, k, _dp(planes), dt, time, nstep))
+
+    def download(self, k: int):
+        planes = np.empty((NPLANES, *self.shapes[k]))
+        dt, t, n = C.c_double(), C.c_double(), C.c_int()
+        _check(lib().athb_batch_download(self._h, k, _dp(planes), C.byref(dt), C.byref(t), C.byref(n)))
+        return planes, dt.value, t.value, n.value
+
+    def prepare(self) -> None:
+        _check(lib().athb_batch_prepare(self._h))
+
+    def run(self, max_steps: int = 1_000_000) -> int:
+        n = C.c_int()
+        _check(lib().athb_batch_run(self._h, max_steps, C.byref(n)))
+        return n.value
+
+    def run_async(self, nsteps: int) -> None:
+        _check(lib().athb_batch_run_async(self._h, nsteps))
+
+    def synchronize(self) -> None:
+        _check(lib().athb_batch_synchronize(self._h))
+
+    @property
+    def stream(self) -> int:
+        return lib().athb_batch_stream(self._h) or 0
+
+    def set_ly(self, k: int, ly: int) -> None:
+        _check(lib().athb_batch_set_ly(self._h, k, ly))
+
+    def commit(self) -> None:
+        _check(lib().athb_batch_commit(self._h))
+
+    def set_grid(self, blocks: int) -> None:
+        _check(lib().athb_batch_set_grid(self._h, blocks))
+
+    @property
+    def grid(self) -> int:
+        return lib().athb_batch_grid(self._h)
+
+    def close(self) -> None:
+        if self._h:
+            lib().athb_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

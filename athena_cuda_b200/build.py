@@ -31,7 +31,7 @@ NVCC_FLAGS = ARCH + [
 CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", f"-I{ROOT / 'include'}",
              f"-I{CUDA_HOME / 'include'}"]
 
-CU_SOURCES = ["athb_core.cu", "athb_dropin.cu"]
+CU_SOURCES = ["athb_core.cu", "athb_dropin.cu", "athb_batch.cu"]
 CPP_SOURCES = ["athinput.cpp", "problems.cpp"]
 HEADERS = ["mhd_physics.cuh", "step_types.cuh", "step_kernels.cuh", "athb_internal.h"]
 
@@ -53,15 +53,20 @@ def _stale(target: Path, deps: list[Path]) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> Path:
-    OBJ.mkdir(exist_ok=True)
+def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False,
+          defines: list[str] = (), lib: Path | None = None, obj: Path | None = None) -> Path:
+    global OBJ
+    lib = lib or LIB
+    OBJ = obj or OBJ
+    OBJ.mkdir(exist_ok=True, parents=True)
     hdrs = [CSRC / h for h in HEADERS] + [ROOT / "include" / "athena_b200.h", Path(__file__)]
     objs = []
     for src in CU_SOURCES:
         o = OBJ / (src + ".o")
         if force or ptxas_info or _stale(o, [CSRC / src] + hdrs):
             extra = ["-Xptxas", "-v"] if ptxas_info else []
-            out = _run([NVCC, *NVCC_FLAGS, *extra, "-c", str(CSRC / src), "-o", str(o)], verbose)
+            out = _run([NVCC, *NVCC_FLAGS, *[f"-D{d}" for d in defines], *extra, "-c", str(CSRC / src),
+                        "-o", str(o)], verbose)
             if ptxas_info:
                 print(out)
         objs.append(o)
@@ -70,9 +75,9 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         if force or _stale(o, [CSRC / src] + hdrs):
             _run(["g++", *CXX_FLAGS, "-c", str(CSRC / src), "-o", str(o)], verbose)
         objs.append(o)
-    if force or _stale(LIB, objs):
-        _run([NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart"], verbose)
-    return LIB
+    if force or _stale(lib, objs):
+        _run([NVCC, *ARCH, "-shared", "-o", str(lib), *map(str, objs), "-lcudart"], verbose)
+    return lib
 
 
 def main() -> None:

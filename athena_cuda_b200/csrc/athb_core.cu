@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -412,17 +413,31 @@ extern "C" int athb_status(athb_ctx* c, double* time, double* dt, int* nstep, in
   return ATHB_OK;
 }
 
+// Launches as many steps as the clock says remain (dt can grow at most 2x per
+// step, so (tlim - time)/dt does not overshoot the end by more than the nlim
+// bound allows), then re-reads the clock, until done or nsteps launched.
 extern "C" int athb_run(athb_ctx* c, int nsteps, int* steps_done) {
   if (!c) return athb_fail(ATHB_ERR_ARG, "null context");
-  StepState before;
-  int rc = athb_read_clock(c, &before);
+  StepState h;
+  int rc = athb_read_clock(c, &h);
   if (rc) return rc;
-  rc = athb_run_async(c, nsteps);
-  if (rc) return rc;
-  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  const int start = h.nstep;
+  long long launched = 0;
+  while (!h.done && launched < nsteps) {
+    double est = (h.tlim - h.time) / h.dt;
+    long long want = est < 1.0 ? 1 : (long long)std::ceil(est);
+    if (h.nlim >= 0) want = std::min<long long>(want, std::max(1, h.nlim - h.nstep));
+    want = std::min<long long>(want, nsteps - launched);
+    rc = athb_run_async(c, (int)want);
+    if (rc) return rc;
+    launched += want;
+    rc = athb_read_clock(c, &h);
+    if (rc) return rc;
+    if (h.flags & kErrNonFinite) break;
+  }
   int nstep = 0;
   rc = athb_status(c, nullptr, nullptr, &nstep, nullptr);
-  if (steps_done) *steps_done = nstep - before.nstep;
+  if (steps_done) *steps_done = nstep - start;
   return rc;
 }
 
@@ -445,6 +460,17 @@ extern "C" int athb_new_dt(athb_ctx* c, double* dt) {
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   return athb_status(c, nullptr, dt, nullptr, nullptr);
 }
+
+// Tuning: rows per y-sweep march segment (any value >= 1 gives the same
+// results; it only changes the work decomposition).
+extern "C" int athb_set_ly(athb_ctx* c, int ly) {
+  if (!c || ly < 1) return athb_fail(ATHB_ERR_ARG, "bad arguments");
+  c->ly = ly;
+  drop_graphs(c);
+  return ATHB_OK;
+}
+
+extern "C" int athb_get_ly(const athb_ctx* c) { return c ? c->ly : 0; }
 
 extern "C" int athb_grid_info_of(const athb_ctx* c, athb_grid_info* g) {
   if (!c || !g) return athb_fail(ATHB_ERR_ARG, "null argument");

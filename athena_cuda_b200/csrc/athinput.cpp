@@ -39,24 +39,51 @@ static std::string trim(const std::string& s) {
   return s.substr(a, b - a);
 }
 
+static int parse_lines(const std::vector<std::string>& lines, const char* path, athb_params** out);
+
+static std::vector<std::string> split_lines(const std::string& text) {
+  std::vector<std::string> v;
+  size_t a = 0;
+  while (a <= text.size()) {
+    size_t b = text.find('\n', a);
+    if (b == std::string::npos) b = text.size();
+    v.push_back(text.substr(a, b - a));
+    a = b + 1;
+  }
+  return v;
+}
+
 extern "C" int athb_params_open(const char* path, athb_params** out) {
   if (!path || !out) return athb_fail(ATHB_ERR_ARG, "null argument");
   *out = nullptr;
   FILE* fp = fopen(path, "r");
   if (!fp) return athb_fail(ATHB_ERR_PARSE, "parameter file %s could not be opened", path);
+  std::vector<std::string> lines;
+  char line[1024];
+  while (fgets(line, sizeof line, fp)) lines.push_back(line);
+  fclose(fp);
+  return parse_lines(lines, path, out);
+}
+
+extern "C" int athb_params_from_string(const char* text, athb_params** out) {
+  if (!text || !out) return athb_fail(ATHB_ERR_ARG, "null argument");
+  *out = nullptr;
+  return parse_lines(split_lines(text), "<string>", out);
+}
+
+static int parse_lines(const std::vector<std::string>& lines, const char* path, athb_params** out) {
   athb_params* p = new athb_params();
   athb_params::Block* cur = nullptr;
-  char line[1024];
   int lineno = 0;
-  while (fgets(line, sizeof line, fp)) {
+  for (const std::string& raw : lines) {
     lineno++;
-    std::string s = trim(line);
+    std::string s = trim(raw);
     if (s.empty() || s[0] == '#') continue;
     if (s.compare(0, 9, "<par_end>") == 0) break;
     if (s[0] == '<') {
       size_t e = s.find('>');
       if (e == std::string::npos) {
-        fclose(fp); delete p;
+        delete p;
         return athb_fail(ATHB_ERR_PARSE, "%s:%d: block name not terminated", path, lineno);
       }
       std::string name = trim(s.substr(1, e - 1));
@@ -65,14 +92,14 @@ extern "C" int athb_params_open(const char* path, athb_params** out) {
       continue;
     }
     if (!cur) {
-      fclose(fp); delete p;
+      delete p;
       return athb_fail(ATHB_ERR_PARSE, "%s:%d: parameter outside any <block>", path, lineno);
     }
     size_t hash = s.find('#');
     std::string body = hash == std::string::npos ? s : s.substr(0, hash);
     size_t eq = body.find('=');
     if (eq == std::string::npos) {
-      fclose(fp); delete p;
+      delete p;
       return athb_fail(ATHB_ERR_PARSE, "%s:%d: no '=' in \"%s\"", path, lineno, s.c_str());
     }
     std::string name = trim(body.substr(0, eq)), value = trim(body.substr(eq + 1));
@@ -80,7 +107,6 @@ extern "C" int athb_params_open(const char* path, athb_params** out) {
     for (auto& q : cur->pars) if (q.name == name) { q.value = value; replaced = true; }
     if (!replaced) cur->pars.push_back({name, value});
   }
-  fclose(fp);
   *out = p;
   return ATHB_OK;
 }

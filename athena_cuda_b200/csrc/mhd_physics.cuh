@@ -435,29 +435,30 @@ ATHB_HD RoeSpeeds roe_speeds(const RoeAvg& r, double b1, const Eos& eos) {
   return s;
 }
 
-// Roe eigenvectors (src/esystem_roe.c:91-291) as distinct entries.
-//   R rows 0,1 have zeros in columns 1 and 5; rows 5,6 have a zero in column 3;
-//   R45=-R41, R54=R52, R55=R51, R56=R50 (row 6 likewise).
-//   L rows 1 and 5 have zeros in columns 1 and 4; L5 = (-L10,.,-L12,-L13,.,L15,L16);
-//   L45=L25, L46=L26, L65=L05, L66=L06.
-struct RoeVec {
-  double af, as;  // alpha_f, alpha_s before normalisation (R row 0)
-  double R10, R12, R13, R14, R16;
-  double R20, R21, R22, R23, R24, R25, R26;
-  double R30, R31, R32, R33, R34, R35, R36;
-  double R40, R41, R42, R43, R44, R46;
-  double R50, R51, R52, R60, R61, R62;
-  double L00, L01, L02, L03, L04, L05, L06;
-  double L10, L12, L13, L15, L16;
-  double L20, L21, L22, L23, L24, L25, L26;
-  double L30, L31, L32, L33, L34, L35, L36;
-  double L40, L41, L42, L43;
-  double L60, L61, L62, L63;
+// Roe eigenvectors (src/esystem_roe.c:91-291), kept as the scalars the 7x7
+// matrices are built from.  Rows of L and columns of R are formed one at a
+// time where they are consumed, so no matrix is ever live in registers.
+//   R columns (n-th right eigenvector), rows 0..6:
+//     c0 = (af, af*ev0, af*v2+qs*b2*, af*v3+qs*b3*, R40, as'*b2*, as'*b3*)
+//     c1 = (0, 0, -b3, b2, R41, -b3*s*isd, b2*s*isd)
+//     c2 = (as, as*ev2, as*v2-qf*b2*, as*v3-qf*b3*, R42, -af'*b2*, -af'*b3*)
+//     c3 = (1, v1, v2, v3, R43, 0, 0)
+//     c4 = (as, as*ev4, as*v2+qf*b2*, as*v3+qf*b3*, R44, -af'*b2*, -af'*b3*)
+//     c5 = (0, 0, b3, -b2, -R41, -b3*s*isd, b2*s*isd)
+//     c6 = (af, af*ev6, af*v2-qs*b2*, af*v3-qs*b3*, R46, as'*b2*, as'*b3*)
+//   L rows: row 5 = (-L10, 0, -L12, -L13, 0, L15, L16) of row 1; rows 2/4 and
+//   0/6 share their last three entries.
+struct RoeScal {
+  double v1, v2, v3, b2, b3, vsq, hp, cf, cs;
+  double af, as, qf, qs;            // alpha_f, alpha_s, qf, qs (right vectors)
+  double bet2, bet3, bet2s, bet3s, vbet, aspbb, afpbb, sgn, isqrtd, sqrtd, asp, afp, gx;
+  double afn, asn, cff, css, qfn, qsn, Afn, Asn, afpb, aspb, q2s, q3s, vqstr, norm2;  // left vectors
 };
 
-ATHB_HD void roe_vectors(const RoeAvg& r, const RoeSpeeds& s, double b1, const Eos& eos,
-                         const double ev[7], RoeVec& V) {
-  const double v1 = r.v1, v2 = r.v2, v3 = r.v3, b2 = r.b2, b3 = r.b3, d = r.droe;
+ATHB_HD void roe_scalars(const RoeAvg& r, const RoeSpeeds& s, double b1, const Eos& eos, RoeScal& S) {
+  const double v2 = r.v2, v3 = r.v3, b2 = r.b2, b3 = r.b3, d = r.droe;
+  S.v1 = r.v1; S.v2 = v2; S.v3 = v3; S.b2 = b2; S.b3 = b3;
+  S.vsq = s.vsq; S.hp = s.hp; S.cf = s.cf; S.cs = s.cs;
   const double bt = sqrt(s.btsq);
   const double bt_star = sqrt(s.bt_starsq);
   double bet2, bet3;
@@ -466,7 +467,8 @@ ATHB_HD void roe_vectors(const RoeAvg& r, const RoeSpeeds& s, double b1, const E
   const double bet2_star = bet2 / sg;
   const double bet3_star = bet3 / sg;
   const double bet_starsq = bet2_star * bet2_star + bet3_star * bet3_star;
-  const double vbet = v2 * bet2_star + v3 * bet3_star;
+  S.bet2 = bet2; S.bet3 = bet3; S.bet2s = bet2_star; S.bet3s = bet3_star;
+  S.vbet = v2 * bet2_star + v3 * bet3_star;
 
   double alpha_f, alpha_s;
   if ((s.cfsq - s.cssq) == 0.0) { alpha_f = 1.0; alpha_s = 0.0; }
@@ -476,125 +478,110 @@ ATHB_HD void roe_vectors(const RoeAvg& r, const RoeSpeeds& s, double b1, const E
     alpha_f = sqrt((s.twid_asq - s.cssq) / (s.cfsq - s.cssq));
     alpha_s = sqrt((s.cfsq - s.twid_asq) / (s.cfsq - s.cssq));
   }
-
   const double sqrtd = sqrt(d);
   const double isqrtd = 1.0 / sqrtd;
   const double sgn = rsign(b1);
   const double twid_a = sqrt(s.twid_asq);
-  double qf = s.cf * alpha_f * sgn;
-  double qs = s.cs * alpha_s * sgn;
+  const double qf = s.cf * alpha_f * sgn;
+  const double qs = s.cs * alpha_s * sgn;
   const double af_prime = twid_a * alpha_f * isqrtd;
   const double as_prime = twid_a * alpha_s * isqrtd;
-  const double afpbb = af_prime * bt_star * bet_starsq;
-  const double aspbb = as_prime * bt_star * bet_starsq;
-  const double hp = s.hp, cf = s.cf, cs = s.cs, vsq = s.vsq;
-
-  V.af = alpha_f; V.as = alpha_s;
-  V.R10 = alpha_f * ev[0]; V.R12 = alpha_s * ev[2]; V.R13 = v1; V.R14 = alpha_s * ev[4]; V.R16 = alpha_f * ev[6];
-  {
-    const double qa = alpha_f * v2, qb = alpha_s * v2, qc = qs * bet2_star, qd = qf * bet2_star;
-    V.R20 = qa + qc; V.R21 = -bet3; V.R22 = qb - qd; V.R23 = v2; V.R24 = qb + qd; V.R25 = bet3; V.R26 = qa - qc;
-  }
-  {
-    const double qa = alpha_f * v3, qb = alpha_s * v3, qc = qs * bet3_star, qd = qf * bet3_star;
-    V.R30 = qa + qc; V.R31 = bet2; V.R32 = qb - qd; V.R33 = v3; V.R34 = qb + qd; V.R35 = -bet2; V.R36 = qa - qc;
-  }
-  V.R40 = alpha_f * (hp - v1 * cf) + qs * vbet + aspbb;
-  V.R41 = -(v2 * bet3 - v3 * bet2);
-  V.R42 = alpha_s * (hp - v1 * cs) - qf * vbet - afpbb;
-  V.R43 = 0.5 * vsq + eos.gamma_2 * r.x / eos.gamma_1;
-  V.R44 = alpha_s * (hp + v1 * cs) + qf * vbet - afpbb;
-  V.R46 = alpha_f * (hp + v1 * cf) - qs * vbet + aspbb;
-  V.R50 = as_prime * bet2_star; V.R51 = -bet3 * sgn * isqrtd; V.R52 = -af_prime * bet2_star;
-  V.R60 = as_prime * bet3_star; V.R61 = bet2 * sgn * isqrtd;  V.R62 = -af_prime * bet3_star;
+  S.af = alpha_f; S.as = alpha_s; S.qf = qf; S.qs = qs;
+  S.afpbb = af_prime * bt_star * bet_starsq;
+  S.aspbb = as_prime * bt_star * bet_starsq;
+  S.sgn = sgn; S.isqrtd = isqrtd; S.sqrtd = sqrtd; S.asp = as_prime; S.afp = af_prime;
+  S.gx = eos.gamma_2 * r.x / eos.gamma_1;
 
   double norm = 0.5 / s.twid_asq;
-  const double cff = norm * alpha_f * cf;
-  const double css = norm * alpha_s * cs;
-  qf *= norm;
-  qs *= norm;
-  const double af = norm * af_prime * d;
-  const double as = norm * as_prime * d;
-  const double afpb = norm * af_prime * bt_star;
-  const double aspb = norm * as_prime * bt_star;
-
+  S.cff = norm * alpha_f * s.cf;
+  S.css = norm * alpha_s * s.cs;
+  S.qfn = qf * norm;
+  S.qsn = qs * norm;
+  S.Afn = norm * af_prime * d;
+  S.Asn = norm * as_prime * d;
+  S.afpb = norm * af_prime * bt_star;
+  S.aspb = norm * as_prime * bt_star;
   norm *= eos.gamma_1;
-  alpha_f *= norm;
-  alpha_s *= norm;
-  const double q2_star = bet2_star / bet_starsq;
-  const double q3_star = bet3_star / bet_starsq;
-  const double vqstr = (v2 * q2_star + v3 * q3_star);
-  norm *= 2.0;
-
-  V.L00 = alpha_f * (vsq - hp) + cff * (cf + v1) - qs * vqstr - aspb;
-  V.L01 = -alpha_f * v1 - cff;
-  V.L02 = -alpha_f * v2 + qs * q2_star;
-  V.L03 = -alpha_f * v3 + qs * q3_star;
-  V.L04 = alpha_f;
-  V.L05 = as * q2_star - alpha_f * b2;
-  V.L06 = as * q3_star - alpha_f * b3;
-
-  V.L10 = 0.5 * (v2 * bet3 - v3 * bet2);
-  V.L12 = -0.5 * bet3;
-  V.L13 = 0.5 * bet2;
-  V.L15 = -0.5 * sqrtd * bet3 * sgn;
-  V.L16 = 0.5 * sqrtd * bet2 * sgn;
-
-  V.L20 = alpha_s * (vsq - hp) + css * (cs + v1) + qf * vqstr + afpb;
-  V.L21 = -alpha_s * v1 - css;
-  V.L22 = -alpha_s * v2 - qf * q2_star;
-  V.L23 = -alpha_s * v3 - qf * q3_star;
-  V.L24 = alpha_s;
-  V.L25 = -af * q2_star - alpha_s * b2;
-  V.L26 = -af * q3_star - alpha_s * b3;
-
-  V.L30 = 1.0 - norm * (0.5 * vsq - eos.gamma_2 * r.x / eos.gamma_1);
-  V.L31 = norm * v1;
-  V.L32 = norm * v2;
-  V.L33 = norm * v3;
-  V.L34 = -norm;
-  V.L35 = norm * b2;
-  V.L36 = norm * b3;
-
-  V.L40 = alpha_s * (vsq - hp) + css * (cs - v1) - qf * vqstr + afpb;
-  V.L41 = -alpha_s * v1 + css;
-  V.L42 = -alpha_s * v2 + qf * q2_star;
-  V.L43 = -alpha_s * v3 + qf * q3_star;
-
-  V.L60 = alpha_f * (vsq - hp) + cff * (cf - v1) + qs * vqstr - aspb;
-  V.L61 = -alpha_f * v1 + cff;
-  V.L62 = -alpha_f * v2 - qs * q2_star;
-  V.L63 = -alpha_f * v3 - qs * q3_star;
+  S.afn = alpha_f * norm;
+  S.asn = alpha_s * norm;
+  S.q2s = bet2_star / bet_starsq;
+  S.q3s = bet3_star / bet_starsq;
+  S.vqstr = (v2 * S.q2s + v3 * S.q3s);
+  S.norm2 = norm * 2.0;
 }
 
-// Column n of the Roe right-eigenmatrix (the n-th right eigenvector).
-ATHB_HD void roe_right_col(const RoeVec& V, int n, double c[7]) {
+// Column n of the Roe right-eigenmatrix.
+ATHB_HD void roe_right_col(const RoeScal& S, const double ev[7], int n, double c[7]) {
   switch (n) {
-  case 0: c[0] = V.af; c[1] = V.R10; c[2] = V.R20; c[3] = V.R30; c[4] = V.R40; c[5] = V.R50; c[6] = V.R60; break;
-  case 1: c[0] = 0.0;  c[1] = 0.0;   c[2] = V.R21; c[3] = V.R31; c[4] = V.R41; c[5] = V.R51; c[6] = V.R61; break;
-  case 2: c[0] = V.as; c[1] = V.R12; c[2] = V.R22; c[3] = V.R32; c[4] = V.R42; c[5] = V.R52; c[6] = V.R62; break;
-  case 3: c[0] = 1.0;  c[1] = V.R13; c[2] = V.R23; c[3] = V.R33; c[4] = V.R43; c[5] = 0.0;   c[6] = 0.0;   break;
-  case 4: c[0] = V.as; c[1] = V.R14; c[2] = V.R24; c[3] = V.R34; c[4] = V.R44; c[5] = V.R52; c[6] = V.R62; break;
-  case 5: c[0] = 0.0;  c[1] = 0.0;   c[2] = V.R25; c[3] = V.R35; c[4] = -V.R41; c[5] = V.R51; c[6] = V.R61; break;
-  default: c[0] = V.af; c[1] = V.R16; c[2] = V.R26; c[3] = V.R36; c[4] = V.R46; c[5] = V.R50; c[6] = V.R60; break;
+  case 0:
+    c[0] = S.af; c[1] = S.af * ev[0]; c[2] = S.af * S.v2 + S.qs * S.bet2s; c[3] = S.af * S.v3 + S.qs * S.bet3s;
+    c[4] = S.af * (S.hp - S.v1 * S.cf) + S.qs * S.vbet + S.aspbb;
+    c[5] = S.asp * S.bet2s; c[6] = S.asp * S.bet3s; break;
+  case 1:
+    c[0] = 0.0; c[1] = 0.0; c[2] = -S.bet3; c[3] = S.bet2; c[4] = -(S.v2 * S.bet3 - S.v3 * S.bet2);
+    c[5] = -S.bet3 * S.sgn * S.isqrtd; c[6] = S.bet2 * S.sgn * S.isqrtd; break;
+  case 2:
+    c[0] = S.as; c[1] = S.as * ev[2]; c[2] = S.as * S.v2 - S.qf * S.bet2s; c[3] = S.as * S.v3 - S.qf * S.bet3s;
+    c[4] = S.as * (S.hp - S.v1 * S.cs) - S.qf * S.vbet - S.afpbb;
+    c[5] = -S.afp * S.bet2s; c[6] = -S.afp * S.bet3s; break;
+  case 3:
+    c[0] = 1.0; c[1] = S.v1; c[2] = S.v2; c[3] = S.v3; c[4] = 0.5 * S.vsq + S.gx; c[5] = 0.0; c[6] = 0.0; break;
+  case 4:
+    c[0] = S.as; c[1] = S.as * ev[4]; c[2] = S.as * S.v2 + S.qf * S.bet2s; c[3] = S.as * S.v3 + S.qf * S.bet3s;
+    c[4] = S.as * (S.hp + S.v1 * S.cs) + S.qf * S.vbet - S.afpbb;
+    c[5] = -S.afp * S.bet2s; c[6] = -S.afp * S.bet3s; break;
+  case 5:
+    c[0] = 0.0; c[1] = 0.0; c[2] = S.bet3; c[3] = -S.bet2; c[4] = (S.v2 * S.bet3 - S.v3 * S.bet2);
+    c[5] = -S.bet3 * S.sgn * S.isqrtd; c[6] = S.bet2 * S.sgn * S.isqrtd; break;
+  default:
+    c[0] = S.af; c[1] = S.af * ev[6]; c[2] = S.af * S.v2 - S.qs * S.bet2s; c[3] = S.af * S.v3 - S.qs * S.bet3s;
+    c[4] = S.af * (S.hp + S.v1 * S.cf) - S.qs * S.vbet + S.aspbb;
+    c[5] = S.asp * S.bet2s; c[6] = S.asp * S.bet3s; break;
   }
 }
 ATHB_HD int roe_right_mask(int n) {  // structural non-zeros of column n
   return (n == 1 || n == 5) ? 0x7C : (n == 3) ? 0x1F : 0x7F;
 }
 
-// a = L * dU (src/flux_roe.c:200-204), terms in column order, zeros skipped.
-ATHB_HD void roe_project(const RoeVec& V, const double u[7], double a[7]) {
-  const double l04 = V.L04 * u[4], l05 = V.L05 * u[5], l06 = V.L06 * u[6];
-  a[0] = V.L00 * u[0] + V.L01 * u[1] + V.L02 * u[2] + V.L03 * u[3] + l04 + l05 + l06;
-  const double p10 = V.L10 * u[0], p12 = V.L12 * u[2], p13 = V.L13 * u[3], p15 = V.L15 * u[5], p16 = V.L16 * u[6];
-  a[1] = p10 + p12 + p13 + p15 + p16;
-  a[5] = -p10 - p12 - p13 + p15 + p16;
-  const double l24 = V.L24 * u[4], l25 = V.L25 * u[5], l26 = V.L26 * u[6];
-  a[2] = V.L20 * u[0] + V.L21 * u[1] + V.L22 * u[2] + V.L23 * u[3] + l24 + l25 + l26;
-  a[3] = V.L30 * u[0] + V.L31 * u[1] + V.L32 * u[2] + V.L33 * u[3] + V.L34 * u[4] + V.L35 * u[5] + V.L36 * u[6];
-  a[4] = V.L40 * u[0] + V.L41 * u[1] + V.L42 * u[2] + V.L43 * u[3] + l24 + l25 + l26;
-  a[6] = V.L60 * u[0] + V.L61 * u[1] + V.L62 * u[2] + V.L63 * u[3] + l04 + l05 + l06;
+// a = L * dU (src/flux_roe.c:200-204), terms in column order, zeros skipped,
+// rows formed in pairs that share entries.
+ATHB_HD void roe_project(const RoeScal& S, const double u[7], double a[7]) {
+  const double vh = S.vsq - S.hp;
+  {  // rows 0 and 6
+    const double p4 = S.afn * u[4];
+    const double p5 = (S.Asn * S.q2s - S.afn * S.b2) * u[5];
+    const double p6 = (S.Asn * S.q3s - S.afn * S.b3) * u[6];
+    a[0] = (S.afn * vh + S.cff * (S.cf + S.v1) - S.qsn * S.vqstr - S.aspb) * u[0] +
+           (-S.afn * S.v1 - S.cff) * u[1] + (-S.afn * S.v2 + S.qsn * S.q2s) * u[2] +
+           (-S.afn * S.v3 + S.qsn * S.q3s) * u[3] + p4 + p5 + p6;
+    a[6] = (S.afn * vh + S.cff * (S.cf - S.v1) + S.qsn * S.vqstr - S.aspb) * u[0] +
+           (-S.afn * S.v1 + S.cff) * u[1] + (-S.afn * S.v2 - S.qsn * S.q2s) * u[2] +
+           (-S.afn * S.v3 - S.qsn * S.q3s) * u[3] + p4 + p5 + p6;
+  }
+  {  // rows 1 and 5
+    const double p0 = (0.5 * (S.v2 * S.bet3 - S.v3 * S.bet2)) * u[0];
+    const double p2 = (-0.5 * S.bet3) * u[2];
+    const double p3 = (0.5 * S.bet2) * u[3];
+    const double p5 = (-0.5 * S.sqrtd * S.bet3 * S.sgn) * u[5];
+    const double p6 = (0.5 * S.sqrtd * S.bet2 * S.sgn) * u[6];
+    a[1] = p0 + p2 + p3 + p5 + p6;
+    a[5] = -p0 - p2 - p3 + p5 + p6;
+  }
+  {  // rows 2 and 4
+    const double p4 = S.asn * u[4];
+    const double p5 = (-S.Afn * S.q2s - S.asn * S.b2) * u[5];
+    const double p6 = (-S.Afn * S.q3s - S.asn * S.b3) * u[6];
+    a[2] = (S.asn * vh + S.css * (S.cs + S.v1) + S.qfn * S.vqstr + S.afpb) * u[0] +
+           (-S.asn * S.v1 - S.css) * u[1] + (-S.asn * S.v2 - S.qfn * S.q2s) * u[2] +
+           (-S.asn * S.v3 - S.qfn * S.q3s) * u[3] + p4 + p5 + p6;
+    a[4] = (S.asn * vh + S.css * (S.cs - S.v1) - S.qfn * S.vqstr + S.afpb) * u[0] +
+           (-S.asn * S.v1 + S.css) * u[1] + (-S.asn * S.v2 + S.qfn * S.q2s) * u[2] +
+           (-S.asn * S.v3 + S.qfn * S.q3s) * u[3] + p4 + p5 + p6;
+  }
+  {  // row 3
+    a[3] = (1.0 - S.norm2 * (0.5 * S.vsq - S.gx)) * u[0] + (S.norm2 * S.v1) * u[1] + (S.norm2 * S.v2) * u[2] +
+           (S.norm2 * S.v3) * u[3] + (-S.norm2) * u[4] + (S.norm2 * S.b2) * u[5] + (S.norm2 * S.b3) * u[6];
+  }
 }
 
 // Physical flux of one side (src/flux_roe.c:136-172).
@@ -616,7 +603,14 @@ ATHB_HD Cons1 side_flux(const Cons1& U, const Prim1& W, double Bxi, double pb) {
 }
 
 // --- src/flux_hlle.c:60-199 ---------------------------------------------------
-ATHB_HD Cons1 flux_hlle(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const Prim1& Wr,
+// Out of line on the device when it is the Roe solver's rare fallback
+// (ATHB_HLLE_NOINLINE), so its code is not replicated at every call site.
+#if defined(__CUDACC__) && defined(ATHB_HLLE_NOINLINE)
+static __host__ __device__ __noinline__ Cons1 flux_hlle(
+#else
+ATHB_HD Cons1 flux_hlle(
+#endif
+const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const Prim1& Wr,
                         double Bxi, const Eos& eos) {
   const RoeAvg r = roe_average(Ul, Ur, Wl, Wr, Bxi);
   const RoeSpeeds s = roe_speeds(r, Bxi, eos);
@@ -690,57 +684,55 @@ ATHB_HD Cons1 flux_roe(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const 
   ev[0] = r.v1 - s.cf; ev[1] = r.v1 - s.vax; ev[2] = r.v1 - s.cs; ev[3] = r.v1;
   ev[4] = r.v1 + s.cs; ev[5] = r.v1 + s.vax; ev[6] = r.v1 + s.cf;
 
-  const Cons1 Fl = side_flux(Ul, Wl, Bxi, r.pbl);
-  const Cons1 Fr = side_flux(Ur, Wr, Bxi, r.pbr);
-
   // Step 5: supersonic faces take the upwind flux.
-  if (ev[0] >= 0.0) return Fl;
-  if (ev[6] <= 0.0) return Fr;
+  if (ev[0] >= 0.0) return side_flux(Ul, Wl, Bxi, r.pbl);
+  if (ev[6] <= 0.0) return side_flux(Ur, Wr, Bxi, r.pbr);
 
-  RoeVec V;
-  roe_vectors(r, s, Bxi, eos, ev, V);
+  RoeScal S;
+  roe_scalars(r, s, Bxi, eos, S);
 
   // Step 6: wave strengths.
-  const double dU[7] = {Ur.d - Ul.d, Ur.mx - Ul.mx, Ur.my - Ul.my, Ur.mz - Ul.mz,
-                        Ur.e - Ul.e, Ur.by - Ul.by, Ur.bz - Ul.bz};
   double a[7];
-  roe_project(V, dU, a);
-
-  // Step 7: positivity of the intermediate states; HLLE if violated.
   {
-    double u[7] = {Ul.d, Ul.mx, Ul.my, Ul.mz, Ul.e, Ul.by, Ul.bz};
-    bool hlle = false;
+    const double dU[7] = {Ur.d - Ul.d, Ur.mx - Ul.mx, Ur.my - Ul.my, Ur.mz - Ul.mz,
+                          Ur.e - Ul.e, Ur.by - Ul.by, Ur.bz - Ul.bz};
+    roe_project(S, dU, a);
+  }
+  // Step 8 starts from the mean of the side fluxes (src/flux_roe.c:252)
+  double F[7];
+  {
+    const Cons1 Fl = side_flux(Ul, Wl, Bxi, r.pbl);
+    const Cons1 Fr = side_flux(Ur, Wr, Bxi, r.pbr);
+    F[0] = 0.5 * (Fl.d + Fr.d); F[1] = 0.5 * (Fl.mx + Fr.mx); F[2] = 0.5 * (Fl.my + Fr.my);
+    F[3] = 0.5 * (Fl.mz + Fr.mz); F[4] = 0.5 * (Fl.e + Fr.e); F[5] = 0.5 * (Fl.by + Fr.by);
+    F[6] = 0.5 * (Fl.bz + Fr.bz);
+  }
+  // Steps 7 and 8 fused over the right eigenvectors: the intermediate states
+  // (positivity test, HLLE on failure) and the Roe flux subtract the same
+  // column n; per component the flux terms keep the reference's order.
+  double u[7] = {Ul.d, Ul.mx, Ul.my, Ul.mz, Ul.e, Ul.by, Ul.bz};
 #pragma unroll
-    for (int n = 0; n < 6; n++) {
-      double c[7];
-      roe_right_col(V, n, c);
+  for (int n = 0; n < 7; n++) {
+    double c[7];
+    roe_right_col(S, ev, n, c);
+    if (n < 6) {
 #pragma unroll
       for (int m = 0; m < 7; m++)
         if ((roe_right_mask(n) >> m) & 1) u[m] += a[n] * c[m];
       if (ev[n + 1] > ev[n]) {
-        if (u[0] <= 0.0) { hlle = true; break; }
-        double p_inter = u[4] - 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0];
-        p_inter -= 0.5 * (u[5] * u[5] + u[6] * u[6] + Bxi * Bxi);
-        if (p_inter < 0.0) { hlle = true; break; }
+        bool bad = (u[0] <= 0.0);
+        if (!bad) {
+          double p_inter = u[4] - 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0];
+          p_inter -= 0.5 * (u[5] * u[5] + u[6] * u[6] + Bxi * Bxi);
+          bad = (p_inter < 0.0);
+        }
+        if (bad) return flux_hlle(Ul, Ur, Wl, Wr, Bxi, eos);
       }
     }
-    if (hlle) return flux_hlle(Ul, Ur, Wl, Wr, Bxi, eos);
-  }
-
-  // Step 8: Roe flux.
-  double coeff[7];
+    const double coeff = 0.5 * rmax(fabs(ev[n]), 0.0) * a[n];
 #pragma unroll
-  for (int m = 0; m < 7; m++) coeff[m] = 0.5 * rmax(fabs(ev[m]), 0.0) * a[m];
-  double F[7] = {0.5 * (Fl.d + Fr.d), 0.5 * (Fl.mx + Fr.mx), 0.5 * (Fl.my + Fr.my),
-                 0.5 * (Fl.mz + Fr.mz), 0.5 * (Fl.e + Fr.e), 0.5 * (Fl.by + Fr.by),
-                 0.5 * (Fl.bz + Fr.bz)};
-#pragma unroll
-  for (int m = 0; m < 7; m++) {
-    double c[7];
-    roe_right_col(V, m, c);
-#pragma unroll
-    for (int n = 0; n < 7; n++)
-      if ((roe_right_mask(m) >> n) & 1) F[n] -= coeff[m] * c[n];
+    for (int k = 0; k < 7; k++)
+      if ((roe_right_mask(n) >> k) & 1) F[k] -= coeff * c[k];
   }
   Cons1 out;
   out.d = F[0]; out.mx = F[1]; out.my = F[2]; out.mz = F[3]; out.e = F[4]; out.by = F[5]; out.bz = F[6];

@@ -178,16 +178,30 @@ __device__ __forceinline__ void predict_y(const GridArgs& g, int bx, int by) {
   }
 }
 
+// Resident blocks per SM the heavy kernels are compiled for (register caps of
+// 168 and 128 per thread): measured faster on B200 than the uncapped 255
+// registers and 2 blocks per SM despite the spills they cause.
+#ifndef ATHB_PREDICT_MINB
+#define ATHB_PREDICT_MINB 3
+#endif
+#ifndef ATHB_CORRECT_MINB
+#define ATHB_CORRECT_MINB 4
+#endif
+
 template <int FLUX>
-__global__ void __launch_bounds__(kThreads) k_predict(GridArgs g, PredictGeom pg) {
-  if (g.st->done) return;
-  int b = blockIdx.x;
+__device__ __forceinline__ void predict_block(const GridArgs& g, const PredictGeom& pg, int b) {
   if (b < pg.nx_blocks) {
     predict_x<FLUX>(g, b % pg.xseg, b / pg.xseg);
   } else {
     b -= pg.nx_blocks;
     predict_y<FLUX>(g, b % pg.ycolblk, b / pg.ycolblk);
   }
+}
+
+template <int FLUX>
+static __global__ void __launch_bounds__(kThreads, ATHB_PREDICT_MINB) k_predict(GridArgs g, PredictGeom pg) {
+  if (g.st->done) return;
+  predict_block<FLUX>(g, pg, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -224,15 +238,19 @@ __device__ __forceinline__ double corner_emf(const GridArgs& g, const double* fx
   return 0.25 * (emf_l1 + emf_r1 + emf_l2 + emf_r2);
 }
 
-// Corner EMF over [i0, i0+ni) x [j0, j0+nj), ni/nj given by the launcher.
-__global__ void __launch_bounds__(kThreads) k_emf(GridArgs g, int i0, int j0, int ni, int nj,
-                                                  int fx_plane, int fy_plane) {
-  if (g.st->done) return;
-  const int t = blockIdx.x * kThreads + threadIdx.x;
+// Corner EMF over [i0, i0+ni) x [j0, j0+nj): work item t.
+__device__ __forceinline__ void emf_item(const GridArgs& g, int i0, int j0, int ni, int nj, int fx_plane,
+                                         int fy_plane, int t) {
   if (t >= ni * nj) return;
   const int j = j0 + t / ni, i = i0 + t % ni;
   g.scr[S_EMF * g.ps + off(g, j, i)] =
       corner_emf(g, g.scr + fx_plane * g.ps, g.scr + fy_plane * g.ps, g.scr + S_ECC * g.ps, j, i);
+}
+
+static __global__ void __launch_bounds__(kThreads) k_emf(GridArgs g, int i0, int j0, int ni, int nj,
+                                                  int fx_plane, int fy_plane) {
+  if (g.st->done) return;
+  emf_item(g, i0, j0, ni, nj, fx_plane, fy_plane, blockIdx.x * kThreads + threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -395,9 +413,7 @@ __device__ __forceinline__ void correct_e(const GridArgs& g, int t, int w) {
 }
 
 template <int FLUX>
-__global__ void __launch_bounds__(kThreads) k_correct(GridArgs g, CorrectGeom cg) {
-  if (g.st->done) return;
-  const int b = blockIdx.x;
+__device__ __forceinline__ void correct_block(const GridArgs& g, const CorrectGeom& cg, int b) {
   if (b < cg.xb) {
     const int t = b * kThreads + threadIdx.x;
     if (t < cg.xw * cg.xn) correct_x<FLUX>(g, t, cg.xw);
@@ -408,6 +424,12 @@ __global__ void __launch_bounds__(kThreads) k_correct(GridArgs g, CorrectGeom cg
     const int t = (b - cg.xb - cg.yb) * kThreads + threadIdx.x;
     if (t < cg.ew * cg.en) correct_e(g, t, cg.ew);
   }
+}
+
+template <int FLUX>
+static __global__ void __launch_bounds__(kThreads, ATHB_CORRECT_MINB) k_correct(GridArgs g, CorrectGeom cg) {
+  if (g.st->done) return;
+  correct_block<FLUX>(g, cg, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -444,11 +466,13 @@ __device__ __forceinline__ void block_max_to(double v, unsigned long long* dst, 
   }
 }
 
+__device__ __forceinline__ double update_cell(const GridArgs& g, int nx1, int ncell, int t);
+
 // ---------------------------------------------------------------------------
 // k_update: CT on the face fields, conservative update, cell-centred B and the
 // per-cell CFL rate.  One thread per interior cell.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_update(GridArgs g, int nx1, int ncell) {
+static __global__ void __launch_bounds__(kThreads) k_update(GridArgs g, int nx1, int ncell) {
   const StepState& st = *g.st;
   const int t = blockIdx.x * kThreads + threadIdx.x;
   if (st.done) {
@@ -463,6 +487,13 @@ __global__ void __launch_bounds__(kThreads) k_update(GridArgs g, int nx1, int nc
     }
     return;
   }
+  block_max_to(update_cell(g, nx1, ncell, t), &g.st->max_dti_bits, &g.st->flags);
+}
+
+// CT, conservative update and cell-centred field of interior cell t; returns
+// the cell's CFL rate (0 for t >= ncell).
+__device__ __forceinline__ double update_cell(const GridArgs& g, int nx1, int ncell, int t) {
+  const StepState& st = *g.st;
   double dti = 0.0;
   if (t < ncell) {
     const int j = g.js + t / nx1, i = g.is + t % nx1;
@@ -512,12 +543,12 @@ __global__ void __launch_bounds__(kThreads) k_update(GridArgs g, int nx1, int nc
     out[P_B3I * ps + o] = b3c;
     dti = cell_dti(d, m1, m2, m3, e, g.eos, g.dx1, g.dx2);
   }
-  block_max_to(dti, &g.st->max_dti_bits, &g.st->flags);
+  return dti;
 }
 
 // Standalone CFL reduction over the interior of the step's input buffer
 // (the reference new_dt(), used before the first step and by the drop-in ABI).
-__global__ void __launch_bounds__(kThreads) k_cfl(GridArgs g, int nx1, int ncell) {
+static __global__ void __launch_bounds__(kThreads) k_cfl(GridArgs g, int nx1, int ncell) {
   const int t = blockIdx.x * kThreads + threadIdx.x;
   double dti = 0.0;
   if (t < ncell) {
@@ -542,8 +573,7 @@ __device__ __forceinline__ void set_step_coeffs(StepState& st, double dx1, doubl
 // initial call (nstep == 0 rule); mode 1: end of a step (time += dt, nstep++
 // first, as src/main.c:268-271).  Then the tlim clamp of the next iteration
 // (src/main.c:230-232) is applied if the loop continues.
-__global__ void k_finalize(StepState* stp, double dx1, double dx2, int mode) {
-  StepState& st = *stp;
+__device__ __forceinline__ void finalize_state(StepState& st, double dx1, double dx2, int mode) {
   if (mode == 1) {
     if (st.done) return;
     st.nstep++;
@@ -559,8 +589,12 @@ __global__ void k_finalize(StepState* stp, double dx1, double dx2, int mode) {
   set_step_coeffs(st, dx1, dx2);
 }
 
+static __global__ void k_finalize(StepState* stp, double dx1, double dx2, int mode) {
+  finalize_state(*stp, dx1, dx2, mode);
+}
+
 // Set dt from the host value without any rule (drop-in integrate_2d path).
-__global__ void k_set_dt(StepState* stp, double dt, double dx1, double dx2) {
+static __global__ void k_set_dt(StepState* stp, double dt, double dx1, double dx2) {
   stp->dt = dt;
   stp->done = 0;
   set_step_coeffs(*stp, dx1, dx2);
@@ -647,9 +681,8 @@ __device__ __forceinline__ bool ghost_src(const GridArgs& g, int kind, int j, in
 
 // Frame enumeration: rows [0,js) and (je,sy) full width, then rows [js,je]
 // columns [0,is) and (ie,sx).  One thread per frame cell handles all planes.
-__global__ void __launch_bounds__(kThreads) k_ghost(GridArgs g, int sx, int sy, int nframe,
-                                                   int mode, int sides) {
-  const int t = blockIdx.x * kThreads + threadIdx.x;
+__device__ __forceinline__ void ghost_item(const GridArgs& g, int sx, int sy, int nframe, int mode, int sides,
+                                           int t) {
   if (t >= nframe) return;
   const int nbot = g.js * sx, ntop = (sy - g.je - 1) * sx;
   int j, i;
@@ -679,6 +712,11 @@ __global__ void __launch_bounds__(kThreads) k_ghost(GridArgs g, int sx, int sy, 
     s[P_B1I * ps + o] = s[P_B1I * ps + off(g, sj, si)];
   if (ghost_src(g, 2, j, i, mode, sides, sj, si, f1, f2))
     s[P_B2I * ps + o] = s[P_B2I * ps + off(g, sj, si)];
+}
+
+static __global__ void __launch_bounds__(kThreads) k_ghost(GridArgs g, int sx, int sy, int nframe, int mode,
+                                                   int sides) {
+  ghost_item(g, sx, sy, nframe, mode, sides, blockIdx.x * kThreads + threadIdx.x);
 }
 
 }  // namespace athb

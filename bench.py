@@ -32,6 +32,8 @@ import tempfile
 import time
 from pathlib import Path
 
+import numpy as np
+
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
@@ -68,6 +70,10 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="field_loop", choices=["field_loop", "ensemble"])
+    ap.add_argument("--ensemble-n", type=int, default=512)
+    ap.add_argument("--seq-sample", type=int, default=0,
+                    help="time sequential single-grid runs on every k-th instance only (0: all)")
     return ap.parse_args()
 
 
@@ -332,10 +338,75 @@ def e2e(a, ath: Path) -> dict:
             "path": "integrate_2d + new_dt + set_bvals drop-in calls on a pinned host Grid"}
 
 
+def ensemble_arm(a) -> None:
+    """Batched ensemble (configs: 512 blast instances, sizes 64..512 per side,
+    per-instance parameters, each to its own t = 0.1): one persistent
+    cooperative launch per step for all instances, against the same instances
+    run one after another with the single-grid stepper."""
+    import torch
+
+    from athena_cuda_b200 import Batch, Grid, Params, autotune, ensemble, problem_state
+
+    items = ensemble.instances(a.ensemble_n, seed=2024)
+    sizes = [(b["grid"]["Nx1"], b["grid"]["Nx2"]) for _, b in items]
+    t0 = time.perf_counter()
+    batch = Batch.from_problems(items)
+    setup_s = time.perf_counter() - t0
+    tune = autotune.tune_batch(batch, sizes, cache=Path(tempfile.gettempdir()) / "athb_ly_tuning.json")
+    stream = torch.cuda.ExternalStream(batch.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    e0.record(stream)
+    launches = batch.run(100000)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    batched_s = time.perf_counter() - w0
+    batched_dev_ms = e0.elapsed_time(e1)
+    finals = [batch.download(k) for k in range(batch.n)]
+    zc = sum(nx1 * nx2 * f[3] for (nx1, nx2), f in zip(sizes, finals))
+    assert all(f[2] == 0.1 for f in finals), "every instance ends at its t = 0.1"
+    batch.close()
+
+    # sequential single-grid runs of the same instances
+    stride = a.seq_sample if a.seq_sample > 0 else 1
+    seq_s, seq_zc, checked = 0.0, 0, 0
+    for k in range(0, len(items), stride):
+        name, blocks = items[k]
+        p = Params.from_blocks(blocks)
+        g = Grid.create(p.config())
+        g.upload(problem_state(name, p))
+        g.set_bvals()
+        g.new_dt()
+        g.ly = tune[autotune.size_class(*sizes[k])]
+        torch.cuda.synchronize()
+        w = time.perf_counter()
+        g.run(100000)
+        seq_s += time.perf_counter() - w
+        planes, dt, t, n = g.download()
+        seq_zc += sizes[k][0] * sizes[k][1] * n
+        if k % 64 == 0:  # bit-exact spot check against the batched result
+            assert np.array_equal(planes, finals[k][0]) and n == finals[k][3]
+            checked += 1
+        g.close()
+    scale = 1.0 if stride == 1 else zc / seq_zc
+    line = {"metric": "ensemble zone-cycles/s (512 blast instances to t=0.1, one persistent launch per step)",
+            "value": zc / batched_s, "unit": UNIT, "n_gpus": 1, "dtype": "f64", "data": "synthetic (seeded blast ensemble)",
+            "config": {"workload": f"blast ensemble n={len(items)} sizes 64..512 per side", "seed": 2024},
+            "zone_cycles": zc, "persistent_launches": launches, "batched_s": batched_s,
+            "batched_device_ms": batched_dev_ms, "setup_s": setup_s,
+            "sequential_s": seq_s * scale, "sequential_zc_per_s": seq_zc / seq_s,
+            "speedup_vs_sequential": (seq_s * scale) / batched_s,
+            "sequential_sample_stride": stride, "bit_exact_spot_checks": checked, "ly_table": tune}
+    print(json.dumps(line))
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         reference_arm(a)
+    elif a.workload == "ensemble":
+        ensemble_arm(a)
     else:
         ours(a)
 

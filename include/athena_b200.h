@@ -141,6 +141,10 @@ int athb_run_async(athb_ctx *ctx, int nsteps);
  * the mean time per step of each kernel in ms_out[7]: predict, emf (half
  * step), correct, emf (full step), update (+CFL), finalize, ghost.          */
 int athb_profile_steps(athb_ctx *ctx, int nsteps, double *ms_out);
+/* Tuning knob: rows per y-sweep march segment (work decomposition only; the
+ * results do not depend on it).                                             */
+int athb_set_ly(athb_ctx *ctx, int ly);
+int athb_get_ly(const athb_ctx *ctx);
 /* The CUDA stream the context launches on (as a cudaStream_t).               */
 void *athb_stream(athb_ctx *ctx);
 
@@ -151,6 +155,8 @@ void athb_host_free(void *p);
 /* ---- athinput (src/par.c format) and problem generators ---------------- */
 typedef struct athb_params athb_params;
 int athb_params_open(const char *path, athb_params **out);
+/* the same from the text of an athinput file                               */
+int athb_params_from_string(const char *text, athb_params **out);
 /* "block/name=value" overrides of existing keys (src/par.c:170-209)         */
 int athb_params_override(athb_params *p, const char *arg);
 int athb_params_getd(const athb_params *p, const char *block, const char *name, double *v);
@@ -186,6 +192,31 @@ int athb_create_from_athinput(const char *path, int noverride, const char *const
  * Userwork_after_loop): err[0]=RMS, err[1..8] = d M1 M2 M3 E B1c B2c B3c,
  * each divided by Nx1*Nx2.  Only for contexts created by cpaw2d.            */
 int athb_cpaw2d_errors(athb_ctx *ctx, double err[9]);
+
+/* ---- batched ensembles ---------------------------------------------------- */
+/* Many independent grids (any sizes, own dt and end time, shared flux and
+ * device) advanced by one persistent cooperative kernel launch per step.
+ * Every instance is bit-identical to a single-grid run of the same problem. */
+typedef struct athb_batch athb_batch;
+int athb_batch_create(int n, const athb_config *cfgs, athb_batch **out);
+void athb_batch_destroy(athb_batch *b);
+int athb_batch_size(const athb_batch *b);
+/* instance state in the athb_upload layout, and its clock                   */
+int athb_batch_upload(athb_batch *b, int k, const double *planes, double dt, double time, int nstep);
+int athb_batch_download(athb_batch *b, int k, double *planes, double *dt, double *time, int *nstep);
+/* set_bvals and the first new_dt of every instance (src/main.c:139-149)      */
+int athb_batch_prepare(athb_batch *b);
+/* steps until every instance is done or max_steps launches                  */
+int athb_batch_run(athb_batch *b, int max_steps, int *launches);
+int athb_batch_run_async(athb_batch *b, int nsteps);
+int athb_batch_synchronize(athb_batch *b);
+void *athb_batch_stream(athb_batch *b);
+/* tuning: y-march segment length of instance k (applied by _commit) and the
+ * number of persistent blocks (at most the co-resident maximum)             */
+int athb_batch_set_ly(athb_batch *b, int k, int ly);
+int athb_batch_commit(athb_batch *b);
+int athb_batch_set_grid(athb_batch *b, int blocks);
+int athb_batch_grid(const athb_batch *b);
 
 /* Drop-in configuration without the host program's par.c.                  */
 void athb_dropin_set_bc(int ibc_x1, int obc_x1, int ibc_x2, int obc_x2);

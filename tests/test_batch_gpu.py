@@ -1,0 +1,77 @@
+"""Batched ensemble: independent grids of different sizes, parameters and
+boundary conditions advanced by one persistent launch per step.  Every
+instance must equal the single-grid stepper and the reference CPU path bit
+for bit, and each must stop at its own end time."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import refutil
+from athena_cuda_b200 import PLANES, Batch, Grid, configs, ensemble, write_athinput
+
+pytestmark = pytest.mark.gpu
+
+
+def _items():
+    items = ensemble.instances(6, seed=7, sizes=(8, 12, 16, 24, 40), tlim=0.06)
+    # different boundary kinds and problems in the same batch
+    items.append(("blast", configs.blast(20, 12, tlim=0.05, bc=(1, 2, 2, 1))))
+    items.append(("field_loop", configs.field_loop(32, 16, tlim=0.04)))
+    items.append(("cpaw2d", configs.cpaw2d(16, 8, tlim=0.05)))
+    return items
+
+
+def test_batch_matches_single_grid_and_reference(tmp_path):
+    items = _items()
+    b = Batch.from_problems(items)
+    launches = b.run(10_000)
+    assert launches > 0
+    results = [b.download(k) for k in range(b.n)]
+    b.close()
+    nsteps = set()
+    for k, (problem, blocks) in enumerate(items):
+        planes, dt, t, n = results[k]
+        assert t == blocks["time"]["tlim"], (k, t)
+        nsteps.add(n)
+        ath = write_athinput(tmp_path / f"a{k}", blocks)
+        g = Grid.from_athinput(ath, problem)
+        g.run(1_000_000)
+        p2, dt2, t2, n2 = g.download()
+        g.close()
+        rep = refutil.mismatch_report(p2, planes, PLANES)
+        assert rep == "", f"instance {k} differs from the single-grid run:\n{rep}"
+        assert (n, t, dt) == (n2, t2, dt2)
+        if refutil.have_ref(problem):
+            ref = refutil.run_ref(problem, "roe", ath, tmp_path)
+            assert refutil.mismatch_report(ref["planes"], planes, PLANES) == ""
+            assert (n, t, dt) == (ref["nstep"], ref["time"], ref["dt"])
+    assert len(nsteps) > 1, "instances should take different numbers of steps"
+
+
+def test_batch_partial_runs_and_tuning_keep_results(tmp_path):
+    """Re-tuned segment lengths and persistent grid sizes change only the
+    schedule: results after the same number of launches are identical."""
+    items = _items()[:5]
+    ref = Batch.from_problems(items)
+    ref.run(12)
+    want = [ref.download(k)[0] for k in range(ref.n)]
+    ref.close()
+    b = Batch.from_problems(items)
+    for k in range(b.n):
+        b.set_ly(k, 4 + 3 * k)
+    b.commit()
+    b.set_grid(37)
+    b.run_async(5)
+    b.synchronize()
+    b.run(7)
+    for k in range(b.n):
+        assert refutil.mismatch_report(want[k], b.download(k)[0], PLANES) == ""
+    b.close()
+
+
+def test_autotuner_returns_a_candidate():
+    from athena_cuda_b200 import autotune
+
+    ly, times = autotune.tune_ly(24, 40, steps=2)
+    assert ly in autotune.LY_CANDIDATES and ly in times and all(t > 0 for t in times.values())
