@@ -31,7 +31,7 @@ NVCC_FLAGS = ARCH + [
 CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", f"-I{ROOT / 'include'}",
              f"-I{CUDA_HOME / 'include'}"]
 
-CU_SOURCES = ["athb_core.cu", "athb_dropin.cu", "athb_batch.cu"]
+CU_SOURCES = ["athb_core.cu", "athb_dropin.cu", "athb_batch.cu", "athb_noalloc.cu"]
 CPP_SOURCES = ["athinput.cpp", "problems.cpp"]
 HEADERS = ["mhd_physics.cuh", "step_types.cuh", "step_kernels.cuh", "athb_internal.h"]
 

@@ -218,6 +218,25 @@ int athb_batch_commit(athb_batch *b);
 int athb_batch_set_grid(athb_batch *b, int blocks);
 int athb_batch_grid(const athb_batch *b);
 
+/* ---- allocation-free step ------------------------------------------------ */
+/* No counterpart in the reference.  One integrate_2d step (the cells
+ * integrate_2d writes) from d_in into d_out, both caller-owned device buffers
+ * in the athb_upload layout ((nx2+8) x (nx1+8) doubles per plane, 11 planes,
+ * ghosts of d_in filled), with time step dt, on `stream` (a cudaStream_t, NULL
+ * for the default stream).  For callers that cannot allocate device memory:
+ * code running while a CUDA graph is captured, programs that reserve the whole
+ * device memory budget up front, allocation-free real-time loops.  It calls
+ * no cudaMalloc/cudaFree: its scratch is a fixed __device__ array in the
+ * library (~2.4 MB, present on every GPU that loads the library until the
+ * process exits), so it accepts only grids with (Nx1+8)*(Nx2+8) <= 5184
+ * (64 x 64, or any shape with as many cells) and rejects larger ones with
+ * ATHB_ERR_ARG.  All calls share that array: calls that overlap on the GPU
+ * race.  The array's device address is looked up on the first call made on
+ * each device (that device current); make that first call before any stream
+ * capture.                                                                  */
+int athb_integrate_noalloc(const athb_config *cfg, const double *d_in, double *d_out, double dt,
+                           void *stream);
+
 /* Drop-in configuration without the host program's par.c.                  */
 void athb_dropin_set_bc(int ibc_x1, int obc_x1, int ibc_x2, int obc_x2);
 void athb_dropin_set_flux(int flux);

@@ -1,0 +1,72 @@
+"""athb_integrate_noalloc: the integrate step for callers that cannot allocate
+device memory -- code that runs while a CUDA graph is being captured, programs
+that reserve the whole device memory budget up front, allocation-free
+real-time loops.  Its scratch is a fixed __device__ array inside the library.
+Checked, through the C ABI, against the drop-in integrate_2d (which uses the
+regular, allocating context) on two consecutive steps: the results must be
+identical value for value."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from athena_cuda_b200 import AthbError, Config, Grid, Params, configs, lib, write_athinput
+from athena_cuda_b200.dropin import HostGrid, _setup_signatures
+
+pytestmark = pytest.mark.gpu
+
+
+def _noalloc():
+    L = lib()
+    f = L.athb_integrate_noalloc
+    f.restype = C.c_int
+    f.argtypes = [C.POINTER(Config), C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]
+    return f
+
+
+def test_noalloc_step_matches_integrate_2d_twice(tmp_path):
+    import torch
+
+    blocks = configs.blast(40, 28)  # (40+8)*(28+8) = 1728 cells, inside the fixed scratch
+    ath = write_athinput(tmp_path / "athinput", blocks)
+    g = Grid.from_athinput(ath, "blast")  # problem, set_bvals, first new_dt
+    planes, dt, _, _ = g.download()
+    g.close()
+    cfg = Params(ath).config()
+
+    # the existing entry point: drop-in integrate_2d on a host Grid
+    Ld = _setup_signatures()
+    C.c_double.in_dll(Ld, "Gamma").value = cfg.gamma
+    C.c_double.in_dll(Ld, "Gamma_1").value = cfg.gamma - 1.0
+    C.c_double.in_dll(Ld, "Gamma_2").value = cfg.gamma - 2.0
+    C.c_double.in_dll(Ld, "CourNo").value = cfg.cour_no
+    Ld.athb_dropin_set_bc(cfg.bc_ix1, cfg.bc_ox1, cfg.bc_ix2, cfg.bc_ox2)
+    hg = HostGrid(planes, (cfg.x1max - cfg.x1min) / cfg.nx1, (cfg.x2max - cfg.x2min) / cfg.nx2,
+                  cfg.x1min, cfg.x2min)
+
+    noalloc = _noalloc()
+    d_in = torch.tensor(planes, device="cuda")
+    d_out = d_in.clone()
+    stream = torch.cuda.current_stream()
+    for step_dt in (dt, 0.9 * dt):
+        rc = noalloc(C.byref(cfg), d_in.data_ptr(), d_out.data_ptr(), step_dt, stream.cuda_stream)
+        assert rc == 0, lib().athb_last_error().decode()
+        stream.synchronize()
+        hg.grid.dt = step_dt
+        Ld.integrate_2d(C.byref(hg.grid))
+        np.testing.assert_array_equal(d_out.cpu().numpy(), hg.planes())
+        d_in, d_out = d_out, d_out.clone()
+    Ld.integrate_destruct_2d()
+    hg.close()
+
+
+def test_noalloc_rejects_grids_beyond_its_scratch(tmp_path):
+    import torch
+
+    cfg = Params.from_blocks(configs.field_loop(80, 64)).config()  # 88*72 cells > 5184
+    buf = torch.zeros(11 * 72 * 88, dtype=torch.float64, device="cuda")
+    out = torch.zeros_like(buf)
+    rc = _noalloc()(C.byref(cfg), buf.data_ptr(), out.data_ptr(), 1e-3, None)
+    assert rc == 1 and b"5184" in lib().athb_last_error()
