@@ -97,9 +97,13 @@ def lib() -> C.CDLL:
             "athb_batch_commit": (I, [P]),
             "athb_batch_set_grid": (I, [P, I]),
             "athb_batch_grid": (I, [P]),
+            "athb_batch_timing": (I, [P, I, dp]),
+            "athb_batch_set_mode": (I, [P, I]),
+            "athb_batch_mode": (I, [P]),
             "athb_profile_steps": (I, [P, I, dp]),
             "athb_fp64_peak": (I, [I, dp]),
             "athb_set_ly": (I, [P, I]),
+            "athb_diagnostics": (I, [P, dp]),
             "athb_get_ly": (I, [P]),
             "athb_host_free": (None, [P]),
         }
@@ -262,6 +266,12 @@ class Grid:
         _check(lib().athb_profile_steps(self._h, nsteps, ms))
         return dict(zip(("predict", "emf_half", "correct", "emf_full", "update_cfl", "finalize", "ghost"), ms))
 
+    def diagnostics(self) -> dict:
+        """Device-side integrals / maxima of the current state."""
+        out = np.zeros(6)
+        _check(lib().athb_diagnostics(self._h, _dp(out)))
+        return dict(zip(("mass", "energy", "emag", "bp2", "max_divb", "max_j3"), out.tolist()))
+
     def cpaw2d_errors(self) -> np.ndarray:
         err = np.zeros(9)
         _check(lib().athb_cpaw2d_errors(self._h, _dp(err)))
@@ -360,6 +370,25 @@ class Batch:
     @property
     def grid(self) -> int:
         return lib().athb_batch_grid(self._h)
+
+    PERSISTENT, PHASED = 0, 1
+
+    @property
+    def mode(self) -> int:
+        """Batch.PERSISTENT (one cooperative launch per step) or Batch.PHASED
+        (one launch per phase); results are identical."""
+        return lib().athb_batch_mode(self._h)
+
+    @mode.setter
+    def mode(self, m: int) -> None:
+        _check(lib().athb_batch_set_mode(self._h, m))
+
+    def timing(self, enable: int = -1) -> dict:
+        """Per-phase ms (enable=1 to start recording, 0 to stop, -1 to just
+        read)."""
+        ms = np.zeros(6)
+        _check(lib().athb_batch_timing(self._h, enable, _dp(ms)))
+        return dict(zip(("predict", "emf_half", "correct", "emf_full", "update_cfl", "ghost_finalize"), ms.tolist()))
 
     def close(self) -> None:
         if self._h:

@@ -4,7 +4,8 @@
 // The persistent kernel walks six phases (predict, half-step corner EMF,
 // correct, full-step corner EMF, update + CFL, ghost fill + finalize); in each
 // phase the blocks of the launch take the (instance, block) work items of all
-// active instances round-robin, and a grid-wide barrier separates the phases.
+// active instances from a shared counter, and a grid-wide barrier separates
+// the phases.
 // The per-item work is the very device code of the single-grid kernels, so
 // every instance is bit-identical to a single-grid run of the same problem.
 //
@@ -49,17 +50,38 @@ struct BarrierState {
   unsigned int gen;
 };
 
+// Units of work: the 128-thread blocks of the single-grid kernels.  A work
+// item is a chunk of up to chunk_of(ph) consecutive units of one instance;
+// item w of phase ph is wmap[mbase[ph] + w].  Chunks amortise the per-item
+// cost (ticket, lookup, barriers) over several units; short units (EMF,
+// update, ghost fill) take longer chunks (chunk_of).
+__host__ __device__ constexpr int chunk_of(int ph) {
+  return ph == 0 ? 2 : ph == 2 ? 2 : ph == 1 || ph == 3 ? 8 : 4;
+}
+
+struct __align__(16) WorkItem {
+  int id, b0, nb, pad;
+};
+
 struct BatchDev {
   const InstGeom* inst;
   StepState* st;
   int* cur;
   unsigned int* ghost_left;
-  const int* off;  // kPhases x (n+1) prefix sums of work items of the active instances
-  const int* ids;  // active instance ids; ids[n] = number active
+  const int* mbase;     // kPhases + 1: start of each phase's items in wmap
+  const WorkItem* wmap;
+  unsigned int* tick;   // kPhases work counters (dynamic item assignment)
   int n;
   BarrierState* bar;
   int* err;
+  unsigned long long* timing;  // optional: ns spent per phase, accumulated by block 0
 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 __device__ __forceinline__ int item_count(const InstGeom& I, int ph) {
   switch (ph) {
@@ -95,69 +117,185 @@ __device__ void grid_barrier(const BatchDev& B) {
   __syncthreads();
 }
 
+// Copy instance k's geometry into shared memory (all threads), with the
+// state buffers swapped when its current state is in the second buffer.
+__device__ __forceinline__ void load_geom(const BatchDev& B, InstGeom& s_I, int k, int cur) {
+  constexpr int kWords = (int)(sizeof(InstGeom) / sizeof(unsigned long long));
+  static_assert(sizeof(InstGeom) % sizeof(unsigned long long) == 0, "InstGeom copy granularity");
+  static_assert(kWords <= kThreads, "InstGeom copy width");
+  if (threadIdx.x < kWords)
+    reinterpret_cast<unsigned long long*>(&s_I)[threadIdx.x] =
+        reinterpret_cast<const unsigned long long*>(&B.inst[k])[threadIdx.x];
+  __syncthreads();
+  if (threadIdx.x == 0 && cur) {
+    const double* a = s_I.g.in;
+    s_I.g.in = s_I.g.out;
+    s_I.g.out = const_cast<double*>(a);
+  }
+  __syncthreads();
+}
+
+// Units b0 .. b0+nb-1 of phase ph of instance k (geometry I).
 template <int FLUX>
-__global__ void __launch_bounds__(kThreads, kBatchMinBlocks) k_batch_step(BatchDev B) {
-  // the current work item's instance data, loaded once per item by thread 0
-  __shared__ InstGeom s_I;
-  __shared__ int s_k, s_b, s_skip;
-  const int na = B.ids[B.n];
-  for (int ph = 0; ph < kPhases; ph++) {
-    const int* off = B.off + ph * (B.n + 1);
-    const int total = off[na];
-    for (int w = blockIdx.x; w < total; w += gridDim.x) {
-      __syncthreads();  // the previous item is finished with s_I
-      if (threadIdx.x == 0) {
-        int lo = 0, hi = na;  // off[lo] <= w < off[hi]
-        while (hi - lo > 1) {
-          const int mid = (lo + hi) >> 1;
-          if (off[mid] <= w) lo = mid; else hi = mid;
-        }
-        const int id = B.ids[lo];
-        s_k = id;
-        s_b = w - off[lo];
-        s_skip = *(volatile int*)&B.st[id].done;
-        if (!s_skip) {
-          s_I = B.inst[id];
-          if (B.cur[id]) {  // the state lives in the second buffer
-            const double* a = s_I.g.in;
-            s_I.g.in = s_I.g.out;
-            s_I.g.out = const_cast<double*>(a);
-          }
-        }
-      }
-      __syncthreads();
-      if (s_skip) continue;  // instance has reached its end time
-      const int k = s_k, b = s_b;
-      const InstGeom& I = s_I;
-      const GridArgs& g = I.g;
-      const int t = b * kThreads + threadIdx.x;
-      switch (ph) {
-      case 0: predict_block<FLUX>(g, I.pg, b); break;
-      case 1: emf_item(g, g.is - 1, g.js - 1, I.nx1 + 3, I.nx2 + 3, S_FX, S_FY, t); break;
-      case 2: correct_block<FLUX>(g, I.cg, b); break;
-      case 3: emf_item(g, g.is, g.js, I.nx1 + 1, I.nx2 + 1, S_FX2, S_FY2, t); break;
-      case 4:
-        block_max_to(update_cell(g, I.nx1, I.nx1 * I.nx2, t), &g.st->max_dti_bits, &g.st->flags);
-        break;
-      default: {
-        ghost_item(g, I.sx, I.sy, I.nframe, 3, 3, t);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-          __threadfence();
-          if (atomicSub(&B.ghost_left[k], 1u) == 1u) {
-            // last ghost item of instance k: end of its step
-            __threadfence();
-            B.ghost_left[k] = (unsigned int)item_count(I, kPhases - 1);
-            finalize_state(B.st[k], g.dx1, g.dx2, 1);
-            B.cur[k] ^= 1;
-            __threadfence();
-          }
-        }
-        break;
-      }
+__device__ __forceinline__ void run_chunk(const BatchDev& B, int ph, int k, int b0, int nb, const InstGeom& I) {
+  const GridArgs& g = I.g;
+  switch (ph) {
+  case 0:
+    for (int u = 0; u < nb; u++) predict_block<FLUX>(g, I.pg, b0 + u);
+    break;
+  case 1:
+    for (int u = 0; u < nb; u++)
+      emf_item(g, g.is - 1, g.js - 1, I.nx1 + 3, I.nx2 + 3, S_FX, S_FY, (b0 + u) * kThreads + threadIdx.x);
+    break;
+  case 2:
+    for (int u = 0; u < nb; u++) correct_block<FLUX>(g, I.cg, b0 + u);
+    break;
+  case 3:
+    for (int u = 0; u < nb; u++)
+      emf_item(g, g.is, g.js, I.nx1 + 1, I.nx2 + 1, S_FX2, S_FY2, (b0 + u) * kThreads + threadIdx.x);
+    break;
+  case 4: {
+    // the CFL rate max over the chunk, then one block reduction (max is
+    // order-independent, so dt is the single-grid value)
+    double m = 0.0;
+    bool bad = false;
+    for (int u = 0; u < nb; u++) {
+      const double v = update_cell(g, I.nx1, I.nx1 * I.nx2, (b0 + u) * kThreads + threadIdx.x);
+      if (!(v >= 0.0) || isinf(v)) bad = true;
+      else m = fmax(m, v);
+    }
+    if (bad) atomicOr(&g.st->flags, kErrNonFinite);
+    block_max_to(m, &g.st->max_dti_bits, &g.st->flags);
+    break;
+  }
+  default: {
+    for (int u = 0; u < nb; u++) ghost_item(g, I.sx, I.sy, I.nframe, 3, 3, (b0 + u) * kThreads + threadIdx.x);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      if (atomicSub(&B.ghost_left[k], (unsigned int)nb) == (unsigned int)nb) {
+        // last ghost unit of instance k: end of its step
+        __threadfence();
+        B.ghost_left[k] = (unsigned int)item_count(I, kPhases - 1);
+        finalize_state(B.st[k], g.dx1, g.dx2, 1);
+        B.cur[k] ^= 1;
+        __threadfence();
       }
     }
+    break;
+  }
+  }
+}
+
+// The persistent kernel: all six phases of a step, grid barriers between
+// them.  In each phase a block takes its items from the phase's counter
+// (dynamic assignment, so long and short items balance as under the hardware
+// block scheduler) one item ahead: the ticket of the next item is requested
+// when an item starts and read when it ends.
+template <int FLUX>
+__global__ void __launch_bounds__(kThreads, kBatchMinBlocks) k_batch_step(BatchDev B) {
+  // the current work item's instance data, loaded when the instance changes
+  __shared__ InstGeom s_I;
+  __shared__ int s_k, s_b, s_nb, s_skip, s_load, s_w;
+  unsigned long long t_phase = (B.timing && blockIdx.x == 0 && threadIdx.x == 0) ? global_ns() : 0ull;
+  int k_prev = -1;  // instance held in s_I
+  int cur_prev = -1;
+  for (int ph = 0; ph < kPhases; ph++) {
+    const int base = B.mbase[ph];
+    const int total = B.mbase[ph + 1] - base;
+    unsigned int* tick = B.tick + ph;
+    if (threadIdx.x == 0) {
+      // every block is past the previous phase: its counter is free again
+      if (blockIdx.x == 0) B.tick[ph == 0 ? kPhases - 1 : ph - 1] = 0u;
+      s_w = (int)atomicAdd(tick, 1u);
+    }
+    __syncthreads();
+    int w = s_w;
+    while (w < total) {
+      unsigned int nxt = 0u;
+      if (threadIdx.x == 0) {
+        nxt = atomicAdd(tick, 1u);
+        const WorkItem it = B.wmap[base + w];
+        s_k = it.id;
+        s_b = it.b0;
+        s_nb = it.nb;
+        s_skip = *(volatile int*)&B.st[it.id].done;
+        const int cur = s_skip ? 0 : *(volatile int*)&B.cur[it.id];
+        s_load = (!s_skip && (it.id != k_prev || cur != cur_prev)) ? (cur + 1) : 0;
+      }
+      __syncthreads();  // S1: the item is known (and every thread has read s_w)
+      if (s_skip) {
+        k_prev = -1;  // instance has reached its end time
+      } else {
+        if (s_load) {
+          load_geom(B, s_I, s_k, s_load - 1);
+          k_prev = s_k;
+          cur_prev = s_load - 1;
+        }
+        run_chunk<FLUX>(B, ph, s_k, s_b, s_nb, s_I);
+      }
+      if (threadIdx.x == 0) s_w = (int)nxt;
+      __syncthreads();  // S2: the item is finished with s_I; the next ticket is visible
+      w = s_w;
+    }
     if (ph < kPhases - 1) grid_barrier(B);
+    if (B.timing && blockIdx.x == 0 && threadIdx.x == 0) {
+      const unsigned long long now = global_ns();
+      atomicAdd(&B.timing[ph], now - t_phase);
+      t_phase = now;
+    }
+  }
+}
+
+// Phased execution: one launch per phase, one work item per block (the
+// hardware block scheduler balances), each phase with the register budget of
+// its single-grid kernel.
+template <int PH>
+struct PhaseBlocks {
+  static constexpr int value = PH == 0 ? kPredictMinBlocks : PH == 2 ? kCorrectMinBlocks : 1;
+};
+
+template <int FLUX, int PH>
+__global__ void __launch_bounds__(kThreads, PhaseBlocks<PH>::value) k_batch_phase(BatchDev B) {
+  __shared__ InstGeom s_I;
+  __shared__ int s_k, s_b, s_nb, s_cur;
+  const int base = B.mbase[PH];
+  if ((int)blockIdx.x >= B.mbase[PH + 1] - base) return;
+  if (threadIdx.x == 0) {
+    const WorkItem it = B.wmap[base + blockIdx.x];
+    s_k = it.id;
+    s_b = it.b0;
+    s_nb = it.nb;
+    s_cur = B.st[it.id].done ? -1 : B.cur[it.id];
+  }
+  __syncthreads();
+  if (s_cur < 0) return;  // instance has reached its end time
+  load_geom(B, s_I, s_k, s_cur);
+  run_chunk<FLUX>(B, PH, s_k, s_b, s_nb, s_I);
+}
+
+// Phase timing of the phased mode: the time since the previous stamp, added
+// to timing[ph] (ph < 0 only sets the stamp); timing[kPhases] holds it.
+__global__ void k_stamp(unsigned long long* timing, int ph) {
+  const unsigned long long now = global_ns();
+  if (ph >= 0) timing[ph] += now - timing[kPhases];
+  timing[kPhases] = now;
+}
+
+// wmap of the active instances: block (a, ph) writes the chunks of active
+// slot a in phase ph.
+__global__ void k_build_map(const InstGeom* inst, const int* off, const int* mbase, const int* ids, int n,
+                            WorkItem* wmap) {
+  const int a = blockIdx.x, ph = blockIdx.y;
+  if (a >= ids[n]) return;
+  const int* o = off + ph * (n + 1);
+  const int i0 = o[a], i1 = o[a + 1];
+  const int id = ids[a];
+  const int units = item_count(inst[id], ph), r = chunk_of(ph);
+  WorkItem* m = wmap + mbase[ph];
+  for (int w = i0 + threadIdx.x; w < i1; w += blockDim.x) {
+    const int b0 = (w - i0) * r;
+    m[w] = WorkItem{id, b0, min(r, units - b0), 0};
   }
 }
 
@@ -174,12 +312,19 @@ struct athb_batch {
   StepState* st = nullptr;
   int* cur = nullptr;
   unsigned int* ghost_left = nullptr;
-  int* off = nullptr;
+  int* off = nullptr;           // kPhases x (n+1) item prefix sums, then mbase (kPhases+1)
+  WorkItem* wmap = nullptr;     // item -> (instance, block), built on the device
+  size_t wmap_cap = 0;
+  unsigned int* tick = nullptr; // kPhases work counters
   int* ids = nullptr;
   std::vector<int> active;     // ids of the instances in the work tables
   InstGeom* dgeom = nullptr;
   BarrierState* bar = nullptr;
   int* err = nullptr;
+  unsigned long long* timing = nullptr;  // per-phase ns (when enabled), then a stamp
+  bool timing_on = false;
+  int mode = ATHB_BATCH_PERSISTENT;
+  int phase_total[kPhases] = {0, 0, 0, 0, 0, 0};  // work items per phase (active set)
   cudaStream_t stream = nullptr;
   int grid = 0;            // persistent blocks
   cudaGraphExec_t graph = nullptr;
@@ -216,12 +361,7 @@ static InstGeom make_geom(const athb_config& c, int ly, double* state0, double* 
   g.eos = Eos{c.gamma, c.gamma - 1.0, c.gamma - 2.0};
   g.bc[0] = c.bc_ix1; g.bc[1] = c.bc_ox1; g.bc[2] = c.bc_ix2; g.bc[3] = c.bc_ox2;
   const int nx1 = c.nx1, nx2 = c.nx2;
-  I.pg.xseg = (nx1 + 3 + kXFacesPerWarp - 1) / kXFacesPerWarp;
-  I.pg.xrowblk = (nx2 + 4 + kXRowsPerBlock - 1) / kXRowsPerBlock;
-  I.pg.nx_blocks = I.pg.xseg * I.pg.xrowblk;
-  I.pg.ycolblk = (nx1 + 4 + kThreads - 1) / kThreads;
-  I.pg.yseg = (nx2 + 3 + ly - 1) / ly;
-  I.pg.ny_blocks = I.pg.ycolblk * I.pg.yseg;
+  I.pg = make_predict_geom(nx1, nx2, ly);
   I.cg.xw = nx1 + 1; I.cg.xn = nx2 + 3;
   I.cg.yw = nx1 + 3; I.cg.yn = nx2 + 1;
   I.cg.ew = nx1 + 3; I.cg.en = nx2 + 3;
@@ -246,36 +386,59 @@ static int host_items(const InstGeom& I, int ph) {
   }
 }
 
+static int host_chunks(const InstGeom& I, int ph) { return (host_items(I, ph) + chunk_of(ph) - 1) / chunk_of(ph); }
+
 static void release(athb_batch* b) {
   if (!b) return;
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->graph) cudaGraphExecDestroy(b->graph);
   cudaFree(b->pool); cudaFree(b->st); cudaFree(b->cur); cudaFree(b->ghost_left); cudaFree(b->off);
-  cudaFree(b->ids);
-  cudaFree(b->dgeom); cudaFree(b->bar); cudaFree(b->err);
+  cudaFree(b->ids); cudaFree(b->wmap); cudaFree(b->tick);
+  cudaFree(b->dgeom); cudaFree(b->bar); cudaFree(b->err); cudaFree(b->timing);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
+}
+
+// The captured step launches; it is captured again on the next run.
+static void drop_graph(athb_batch* b) {
+  if (b->graph) {
+    cudaStreamSynchronize(b->stream);
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  b->graph_tried = false;
 }
 
 // Work-item tables over the active instances (b->active).  The graph reads
 // the tables through fixed device pointers, so it stays valid.
 static int upload_work(athb_batch* b) {
   const int n = b->n, na = (int)b->active.size();
-  std::vector<int> off((size_t)kPhases * (n + 1), 0);
+  std::vector<int> off((size_t)kPhases * (n + 1) + kPhases + 1, 0);
+  int* mbase = off.data() + (size_t)kPhases * (n + 1);
   for (int ph = 0; ph < kPhases; ph++) {
     int acc = 0;
     for (int a = 0; a < na; a++) {
       off[(size_t)ph * (n + 1) + a] = acc;
-      acc += host_items(b->geom[b->active[a]], ph);
+      acc += host_chunks(b->geom[b->active[a]], ph);
     }
     off[(size_t)ph * (n + 1) + na] = acc;
+    mbase[ph + 1] = mbase[ph] + acc;
+    b->phase_total[ph] = acc;
   }
+  if ((size_t)mbase[kPhases] > b->wmap_cap)
+    return athb_fail(ATHB_ERR_STATE, "work map capacity %zu < %d items", b->wmap_cap, mbase[kPhases]);
   std::vector<int> ids(n + 1, 0);
   for (int a = 0; a < na; a++) ids[a] = b->active[a];
   ids[n] = na;
+  if (b->mode == ATHB_BATCH_PHASED) drop_graph(b);  // its launches hold the per-phase grid sizes
   CUDA_TRY(cudaMemcpyAsync(b->off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
   CUDA_TRY(cudaMemcpyAsync(b->ids, ids.data(), ids.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  if (na > 0) {
+    k_build_map<<<dim3(na, kPhases), kThreads, 0, b->stream>>>(b->dgeom, b->off, b->off + (size_t)kPhases * (n + 1),
+                                                                b->ids, n, b->wmap);
+    CUDA_TRY(cudaGetLastError());
+  }
   CUDA_TRY(cudaStreamSynchronize(b->stream));
   return ATHB_OK;
 }
@@ -290,6 +453,17 @@ static int upload_tables(athb_batch* b) {
   if (b->active.empty()) {
     b->active.resize(n);
     for (int k = 0; k < n; k++) b->active[k] = k;
+  }
+  size_t items = 0;  // every instance active: the largest map
+  for (int k = 0; k < n; k++)
+    for (int ph = 0; ph < kPhases; ph++) items += (size_t)host_chunks(b->geom[k], ph);
+  if (items > b->wmap_cap) {
+    drop_graph(b);
+    cudaFree(b->wmap);
+    b->wmap = nullptr;
+    b->wmap_cap = 0;
+    CUDA_TRY(cudaMalloc(&b->wmap, items * sizeof(WorkItem)));
+    b->wmap_cap = items;
   }
   return upload_work(b);
 }
@@ -326,11 +500,15 @@ extern "C" int athb_batch_create(int n, const athb_config* cfgs, athb_batch** ou
   if (e == cudaSuccess) e = cudaMalloc(&b->st, n * sizeof(StepState));
   if (e == cudaSuccess) e = cudaMalloc(&b->cur, n * sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc(&b->ghost_left, n * sizeof(unsigned int));
-  if (e == cudaSuccess) e = cudaMalloc(&b->off, (size_t)kPhases * (n + 1) * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&b->off, ((size_t)kPhases * (n + 1) + kPhases + 1) * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&b->tick, kPhases * sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->tick, 0, kPhases * sizeof(unsigned int), b->stream);
   if (e == cudaSuccess) e = cudaMalloc(&b->ids, (size_t)(n + 1) * sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc(&b->dgeom, n * sizeof(InstGeom));
   if (e == cudaSuccess) e = cudaMalloc(&b->bar, sizeof(BarrierState));
   if (e == cudaSuccess) e = cudaMalloc(&b->err, sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&b->timing, (kPhases + 1) * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->timing, 0, (kPhases + 1) * sizeof(unsigned long long), b->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(b->pool, 0, total * sizeof(double), b->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(b->cur, 0, n * sizeof(int), b->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(b->bar, 0, sizeof(BarrierState), b->stream);
@@ -438,6 +616,7 @@ extern "C" int athb_batch_download(athb_batch* b, int k, double* planes, double*
 extern "C" int athb_batch_prepare(athb_batch* b) {
   if (!b) return athb_fail(ATHB_ERR_ARG, "null batch");
   CUDA_TRY(cudaSetDevice(b->device));
+  CUDA_TRY(cudaMemsetAsync(b->tick, 0, kPhases * sizeof(unsigned int), b->stream));
   std::vector<int> cur(b->n);
   CUDA_TRY(cudaMemcpy(cur.data(), b->cur, b->n * sizeof(int), cudaMemcpyDeviceToHost));
   for (int k = 0; k < b->n; k++) {
@@ -456,11 +635,41 @@ extern "C" int athb_batch_prepare(athb_batch* b) {
   return ATHB_OK;
 }
 
-static int launch_step(athb_batch* b) {
+static BatchDev batch_dev(const athb_batch* b) {
   BatchDev D;
-  D.inst = b->dgeom; D.st = b->st; D.cur = b->cur; D.ghost_left = b->ghost_left; D.off = b->off;
-  D.ids = b->ids;
+  D.inst = b->dgeom; D.st = b->st; D.cur = b->cur; D.ghost_left = b->ghost_left;
+  D.mbase = b->off + (size_t)kPhases * (b->n + 1);
+  D.wmap = b->wmap;
+  D.tick = b->tick;
   D.n = b->n; D.bar = b->bar; D.err = b->err;
+  D.timing = b->timing_on ? b->timing : nullptr;
+  return D;
+}
+
+template <int FLUX, int PH>
+static cudaError_t launch_phase(const athb_batch* b, const BatchDev& D) {
+  if (b->phase_total[PH] > 0) k_batch_phase<FLUX, PH><<<b->phase_total[PH], kThreads, 0, b->stream>>>(D);
+  if (b->timing_on) k_stamp<<<1, 1, 0, b->stream>>>(b->timing, PH);
+  return cudaGetLastError();
+}
+
+template <int FLUX>
+static int launch_phases(const athb_batch* b) {
+  const BatchDev D = batch_dev(b);
+  if (b->timing_on) k_stamp<<<1, 1, 0, b->stream>>>(b->timing, -1);
+  CUDA_TRY((launch_phase<FLUX, 0>(b, D)));
+  CUDA_TRY((launch_phase<FLUX, 1>(b, D)));
+  CUDA_TRY((launch_phase<FLUX, 2>(b, D)));
+  CUDA_TRY((launch_phase<FLUX, 3>(b, D)));
+  CUDA_TRY((launch_phase<FLUX, 4>(b, D)));
+  CUDA_TRY((launch_phase<FLUX, 5>(b, D)));
+  return ATHB_OK;
+}
+
+static int launch_step(athb_batch* b) {
+  if (b->mode == ATHB_BATCH_PHASED)
+    return b->flux == ATHB_FLUX_HLLE ? launch_phases<kFluxHlle>(b) : launch_phases<kFluxRoe>(b);
+  BatchDev D = batch_dev(b);
   void* args[] = {&D};
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(b->grid);
@@ -478,8 +687,9 @@ static int launch_step(athb_batch* b) {
   return ATHB_OK;
 }
 
-// Launch nsteps persistent steps (one cooperative launch each; captured in a
-// CUDA graph when the driver allows it) without synchronising.
+// Launch nsteps steps (persistent: one cooperative launch each; phased: six
+// launches each; captured in a CUDA graph when the driver allows it) without
+// synchronising.
 extern "C" int athb_batch_run_async(athb_batch* b, int nsteps) {
   if (!b || nsteps < 0) return athb_fail(ATHB_ERR_ARG, "bad arguments");
   CUDA_TRY(cudaSetDevice(b->device));
@@ -561,4 +771,34 @@ extern "C" int athb_batch_synchronize(athb_batch* b) {
 
 extern "C" void* athb_batch_stream(athb_batch* b) { return b ? (void*)b->stream : nullptr; }
 
+// Per-phase timing of the persistent kernel (block 0's view: each phase ends
+// at the grid barrier): enable, then read ns accumulated per phase.
+extern "C" int athb_batch_timing(athb_batch* b, int enable, double* ms_out) {
+  if (!b) return athb_fail(ATHB_ERR_ARG, "null batch");
+  if (ms_out) {
+    unsigned long long t[kPhases];
+    CUDA_TRY(cudaMemcpyAsync(t, b->timing, sizeof t, cudaMemcpyDeviceToHost, b->stream));
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    for (int k = 0; k < kPhases; k++) ms_out[k] = 1e-6 * (double)t[k];
+  }
+  if (enable >= 0 && (enable != 0) != b->timing_on) {
+    b->timing_on = enable != 0;
+    CUDA_TRY(cudaMemsetAsync(b->timing, 0, (kPhases + 1) * sizeof(unsigned long long), b->stream));
+    drop_graph(b);
+  }
+  return ATHB_OK;
+}
+
 extern "C" int athb_batch_grid(const athb_batch* b) { return b ? b->grid : 0; }
+
+// Execution mode: ATHB_BATCH_PERSISTENT (one cooperative launch per step) or
+// ATHB_BATCH_PHASED (one launch per phase).  Results are identical.
+extern "C" int athb_batch_set_mode(athb_batch* b, int mode) {
+  if (!b || (mode != ATHB_BATCH_PERSISTENT && mode != ATHB_BATCH_PHASED))
+    return athb_fail(ATHB_ERR_ARG, "bad arguments");
+  CUDA_TRY(cudaSetDevice(b->device));
+  b->mode = mode;
+  drop_graph(b);
+  return ATHB_OK;
+}
+extern "C" int athb_batch_mode(const athb_batch* b) { return b ? b->mode : -1; }

@@ -265,15 +265,10 @@ int athb_launch_integrate_split(athb_ctx* c, int from, cudaEvent_t* ev) {
 #define MARK(k) do { if (ev) CUDA_TRY(cudaEventRecord(ev[k], c->stream)); } while (0)
   GridArgs g = grid_args(c, from);
   const int nx1 = c->cfg.nx1, nx2 = c->cfg.nx2;
-  PredictGeom pg;
-  pg.xseg = (nx1 + 3 + kXFacesPerWarp - 1) / kXFacesPerWarp;   // faces [is-1, ie+2]
-  pg.xrowblk = (nx2 + 4 + kXRowsPerBlock - 1) / kXRowsPerBlock;  // rows [js-2, je+2]
-  pg.nx_blocks = pg.xseg * pg.xrowblk;
-  pg.ycolblk = (nx1 + 4 + kThreads - 1) / kThreads;             // columns [is-2, ie+2]
-  pg.yseg = (nx2 + 3 + c->ly - 1) / c->ly;                      // faces [js-1, je+2]
-  pg.ny_blocks = pg.ycolblk * pg.yseg;
+  const PredictGeom pg = make_predict_geom(nx1, nx2, c->ly);
+  const bool hlle = c->cfg.flux == ATHB_FLUX_HLLE;
   MARK(0);
-  if (c->cfg.flux == ATHB_FLUX_HLLE)
+  if (hlle)
     k_predict<kFluxHlle><<<pg.nx_blocks + pg.ny_blocks, kThreads, 0, c->stream>>>(g, pg);
   else
     k_predict<kFluxRoe><<<pg.nx_blocks + pg.ny_blocks, kThreads, 0, c->stream>>>(g, pg);
@@ -292,7 +287,7 @@ int athb_launch_integrate_split(athb_ctx* c, int from, cudaEvent_t* ev) {
   cg.yb = blocks_for((long long)cg.yw * cg.yn);
   cg.eb = blocks_for((long long)cg.ew * cg.en);
   MARK(2);
-  if (c->cfg.flux == ATHB_FLUX_HLLE)
+  if (hlle)
     k_correct<kFluxHlle><<<cg.xb + cg.yb + cg.eb, kThreads, 0, c->stream>>>(g, cg);
   else
     k_correct<kFluxRoe><<<cg.xb + cg.yb + cg.eb, kThreads, 0, c->stream>>>(g, cg);
@@ -530,5 +525,81 @@ extern "C" int athb_fp64_peak(int device, double* ops_per_s) {
   cudaEventDestroy(e1);
   cudaFree(out);
   *ops_per_s = best;
+  return ATHB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Diagnostics of the resident state (interior cells): volume integrals of
+// d, E, the magnetic energy (B1c^2+B2c^2+B3c^2)/2 and of Bp2 = B1c^2+B2c^2
+// (the field-loop output expression, src/field_loop.c:167-171), and the
+// maxima of |div B| from the face fields (the CT invariant) and of |J3|
+// (src/field_loop.c:161-165).  Two deterministic passes: per-block partials
+// into the scratch planes (free between steps), then one block sums them in
+// a fixed order, so a result is the same on every run.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kDiag = 6;  // mass, energy, emag, bp2, max|divB|, max|J3|
+
+__global__ void __launch_bounds__(kThreads) k_diag_partial(GridArgs g, int nx1, int ncell, double* part) {
+  const int t = blockIdx.x * kThreads + threadIdx.x;
+  double v[kDiag] = {0, 0, 0, 0, 0, 0};
+  if (t < ncell) {
+    const int j = g.js + t / nx1, i = g.is + t % nx1;
+    const long long ps = g.ps, o = off(g, j, i), P = g.pitch;
+    const double* s = g.in;
+    const double dv = g.dx1 * g.dx2;
+    const double b1 = s[P_B1C * ps + o], b2 = s[P_B2C * ps + o], b3 = s[P_B3C * ps + o];
+    v[0] = s[P_D * ps + o] * dv;
+    v[1] = s[P_E * ps + o] * dv;
+    v[2] = 0.5 * (b1 * b1 + b2 * b2 + b3 * b3) * dv;
+    v[3] = (b1 * b1 + b2 * b2) * dv;
+    v[4] = fabs((s[P_B1I * ps + o + 1] - s[P_B1I * ps + o]) / g.dx1 +
+                (s[P_B2I * ps + o + P] - s[P_B2I * ps + o]) / g.dx2);
+    v[5] = fabs((s[P_B2I * ps + o] - s[P_B2I * ps + o - 1]) / g.dx1 -
+                (s[P_B1I * ps + o] - s[P_B1I * ps + o - P]) / g.dx2);
+  }
+  __shared__ double red[kThreads / 32][kDiag];
+#pragma unroll
+  for (int k = 0; k < kDiag; k++) {
+    double x = v[k];
+    for (int d = 16; d > 0; d >>= 1) {
+      const double y = __shfl_xor_sync(0xffffffffu, x, d);
+      x = k < 4 ? x + y : fmax(x, y);
+    }
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][k] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < kDiag) {
+    const int k = threadIdx.x;
+    double x = red[0][k];
+    for (int w = 1; w < kThreads / 32; w++) x = k < 4 ? x + red[w][k] : fmax(x, red[w][k]);
+    part[(size_t)blockIdx.x * kDiag + k] = x;
+  }
+}
+
+__global__ void k_diag_final(const double* part, int nblocks, double* out) {
+  if (threadIdx.x < kDiag) {
+    const int k = threadIdx.x;
+    double x = 0.0;
+    for (int b = 0; b < nblocks; b++) x = k < 4 ? x + part[(size_t)b * kDiag + k] : fmax(x, part[(size_t)b * kDiag + k]);
+    out[k] = x;
+  }
+}
+}  // namespace
+
+extern "C" int athb_diagnostics(athb_ctx* c, double out[6]) {
+  if (!c || !out) return athb_fail(ATHB_ERR_ARG, "null argument");
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  GridArgs g = grid_args(c, c->cur);
+  const int n = c->cfg.nx1 * c->cfg.nx2;
+  const int nb = blocks_for(n);
+  double* part = c->scr;                   // scratch planes are free between steps
+  double* res = c->scr + (size_t)nb * kDiag;
+  if ((size_t)(nb + 1) * kDiag > (size_t)c->ps * NSCRATCH) return athb_fail(ATHB_ERR_ARG, "grid too small");
+  k_diag_partial<<<nb, kThreads, 0, c->stream>>>(g, c->cfg.nx1, n, part);
+  k_diag_final<<<1, 32, 0, c->stream>>>(part, nb, res);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemcpyAsync(out, res, kDiag * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
   return ATHB_OK;
 }

@@ -116,13 +116,7 @@ extern "C" int athb_integrate_noalloc(const athb_config* cfg, const double* d_in
 
   k_noalloc_begin<<<1, 1, 0, s>>>(gs.st, dt, gs.dx1, gs.dx2);
 
-  PredictGeom pg;
-  pg.xseg = (nx1 + 3 + kXFacesPerWarp - 1) / kXFacesPerWarp;
-  pg.xrowblk = (nx2 + 4 + kXRowsPerBlock - 1) / kXRowsPerBlock;
-  pg.nx_blocks = pg.xseg * pg.xrowblk;
-  pg.ycolblk = (nx1 + 4 + kThreads - 1) / kThreads;
-  pg.yseg = (nx2 + 3 + gs.ly - 1) / gs.ly;
-  pg.ny_blocks = pg.ycolblk * pg.yseg;
+  const PredictGeom pg = make_predict_geom(nx1, nx2, gs.ly);
   if (cfg->flux == ATHB_FLUX_HLLE) k_predict<kFluxHlle><<<pg.nx_blocks + pg.ny_blocks, kThreads, 0, s>>>(gs, pg);
   else k_predict<kFluxRoe><<<pg.nx_blocks + pg.ny_blocks, kThreads, 0, s>>>(gs, pg);
   k_emf<<<blocks_of((long long)(nx1 + 3) * (nx2 + 3)), kThreads, 0, s>>>(gs, gs.is - 1, gs.js - 1, nx1 + 3, nx2 + 3,

@@ -603,14 +603,7 @@ ATHB_HD Cons1 side_flux(const Cons1& U, const Prim1& W, double Bxi, double pb) {
 }
 
 // --- src/flux_hlle.c:60-199 ---------------------------------------------------
-// Out of line on the device when it is the Roe solver's rare fallback
-// (ATHB_HLLE_NOINLINE), so its code is not replicated at every call site.
-#if defined(__CUDACC__) && defined(ATHB_HLLE_NOINLINE)
-static __host__ __device__ __noinline__ Cons1 flux_hlle(
-#else
-ATHB_HD Cons1 flux_hlle(
-#endif
-const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const Prim1& Wr,
+ATHB_HD Cons1 flux_hlle(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const Prim1& Wr,
                         double Bxi, const Eos& eos) {
   const RoeAvg r = roe_average(Ul, Ur, Wl, Wr, Bxi);
   const RoeSpeeds s = roe_speeds(r, Bxi, eos);

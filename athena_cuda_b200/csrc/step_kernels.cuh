@@ -89,10 +89,26 @@ constexpr int kThreads = 128;
 constexpr int kXRowsPerBlock = kThreads / 32;   // role X: one warp per row segment
 constexpr int kXFacesPerWarp = 31;              // 32 PLM cells -> 31 faces
 
+// Role X: a warp per 31-face row segment, four rows per block.  Role Y: one
+// thread per (column, segment of ly faces), flattened column-fastest over
+// the blocks so that narrow grids leave no idle columns.
 struct PredictGeom {
   int xseg, xrowblk, nx_blocks;  // role X blocks = xseg * xrowblk
-  int ycolblk, yseg, ny_blocks;  // role Y blocks = ycolblk * yseg
+  int ycols, yseg, ny_blocks;    // role Y threads = ycols * yseg, in ny_blocks blocks
 };
+
+// Faces [is-1, ie+2] x rows [js-2, je+2] (role X) and columns [is-2, ie+2]
+// x faces [js-1, je+2] (role Y) of an nx1 x nx2 interior.
+inline PredictGeom make_predict_geom(int nx1, int nx2, int ly) {
+  PredictGeom pg;
+  pg.xseg = (nx1 + 3 + kXFacesPerWarp - 1) / kXFacesPerWarp;
+  pg.xrowblk = (nx2 + 4 + kXRowsPerBlock - 1) / kXRowsPerBlock;
+  pg.nx_blocks = pg.xseg * pg.xrowblk;
+  pg.ycols = nx1 + 4;
+  pg.yseg = (nx2 + 3 + ly - 1) / ly;
+  pg.ny_blocks = (int)(((long long)pg.ycols * pg.yseg + kThreads - 1) / kThreads);
+  return pg;
+}
 
 // ---------------------------------------------------------------------------
 // k_predict: predictor L/R states and fluxes of both sweeps.
@@ -129,10 +145,9 @@ __device__ __forceinline__ void predict_x(const GridArgs& g, int bx, int by) {
     // step 1e (src/__integrate_2d__.c:172-180)
     const Cons1 ul = prim_to_cons(wl, b1l, g.eos);
     const Cons1 ur = prim_to_cons(wrt, b1l, g.eos);
-    const Cons1 f = riemann<FLUX>(ul, ur, wl, wrt, b1l, g.eos);
     store_cons(g.scr + S_ULX * g.ps, g.ps, o, ul);
     store_cons(g.scr + S_URX * g.ps, g.ps, o, ur);
-    store_cons(g.scr + S_FX * g.ps, g.ps, o, f);
+    store_cons(g.scr + S_FX * g.ps, g.ps, o, riemann<FLUX>(ul, ur, wl, wrt, b1l, g.eos));
   }
   // step 3: emf3_cc at t^n on [is-2,ie+2] x [js-2,je+2] (src/__integrate_2d__.c:249-255)
   if ((lane >= 1 || bx == 0) && c <= g.ie + 2) {
@@ -141,23 +156,44 @@ __device__ __forceinline__ void predict_x(const GridArgs& g, int bx, int by) {
   }
 }
 
+// The y role carries three cell states and one face state from row to row;
+// they live in a per-thread ring in shared memory rather than in registers.
+__device__ __forceinline__ void sh_store(double* sh, int slot, int tid, const Prim1& w) {
+  double* p = sh + slot * 7 * kThreads + tid;
+  p[0 * kThreads] = w.d; p[1 * kThreads] = w.vx; p[2 * kThreads] = w.vy; p[3 * kThreads] = w.vz;
+  p[4 * kThreads] = w.p; p[5 * kThreads] = w.by; p[6 * kThreads] = w.bz;
+}
+__device__ __forceinline__ Prim1 sh_load(const double* sh, int slot, int tid) {
+  const double* p = sh + slot * 7 * kThreads + tid;
+  Prim1 w;
+  w.d = p[0 * kThreads]; w.vx = p[1 * kThreads]; w.vy = p[2 * kThreads]; w.vz = p[3 * kThreads];
+  w.p = p[4 * kThreads]; w.by = p[5 * kThreads]; w.bz = p[6 * kThreads];
+  return w;
+}
+
 template <int FLUX>
-__device__ __forceinline__ void predict_y(const GridArgs& g, int bx, int by) {
+__device__ __forceinline__ void predict_y(const GridArgs& g, const PredictGeom& pg, int b) {
+  // slots 0..2: prims of rows k-1, k, k+1 (ring); slot 3: W_L of face k
+  __shared__ double sh[4 * 7 * kThreads];
   const StepState& st = *g.st;
-  const int i = g.is - 2 + bx * kThreads + threadIdx.x;
-  if (i > g.ie + 2) return;
-  const int ja = g.js - 1 + by * g.ly;
+  const int tid = threadIdx.x;
+  const int T = b * kThreads + tid;
+  if (T >= pg.ycols * pg.yseg) return;
+  const int i = g.is - 2 + T % pg.ycols;
+  const int ja = g.js - 1 + (T / pg.ycols) * g.ly;
   const int jb = min(ja + g.ly - 1, g.je + 2);
   const double* s = g.in;
 
-  Prim1 wa = prim_y(g, s, off(g, ja - 2, i));
-  Prim1 wb = prim_y(g, s, off(g, ja - 1, i));
-  Prim1 wl_prev;
+  sh_store(sh, 0, tid, prim_y(g, s, off(g, ja - 2, i)));
+  sh_store(sh, 1, tid, prim_y(g, s, off(g, ja - 1, i)));
+  int r0 = 0;  // ring slot of row k-1
   for (int k = ja - 1; k <= jb; k++) {
     const long long o = off(g, k, i);
-    const Prim1 wc = prim_y(g, s, o + g.pitch);
+    const int r1 = r0 == 2 ? 0 : r0 + 1, r2 = r1 == 2 ? 0 : r1 + 1;
+    sh_store(sh, r2, tid, prim_y(g, s, o + g.pitch));
     Prim1 wln, wrt;
-    plm_cell(wa, wb, wc, s[P_B2C * g.ps + o], st.dtodx2, g.eos, wln, wrt);
+    plm_cell(sh_load(sh, r0, tid), sh_load(sh, r1, tid), sh_load(sh, r2, tid), s[P_B2C * g.ps + o],
+             st.dtodx2, g.eos, wln, wrt);
     // "MHD source terms" for 0.5*dt (src/__integrate_2d__.c:216-224)
     const double b2l = s[P_B2I * g.ps + o], b2r = s[P_B2I * g.ps + o + g.pitch];
     const double src = (s[P_M1 * g.ps + o] / s[P_D * g.ps + o]) * (b2r - b2l) / g.dx2;
@@ -165,41 +201,40 @@ __device__ __forceinline__ void predict_y(const GridArgs& g, int bx, int by) {
     wrt.bz += st.hdt * src;
     if (k >= ja) {
       // step 2e (src/__integrate_2d__.c:233-241)
-      const Cons1 ul = prim_to_cons(wl_prev, b2l, g.eos);
+      const Prim1 wl = sh_load(sh, 3, tid);
+      const Cons1 ul = prim_to_cons(wl, b2l, g.eos);
       const Cons1 ur = prim_to_cons(wrt, b2l, g.eos);
-      const Cons1 f = riemann<FLUX>(ul, ur, wl_prev, wrt, b2l, g.eos);
       store_cons(g.scr + S_ULY * g.ps, g.ps, o, ul);
       store_cons(g.scr + S_URY * g.ps, g.ps, o, ur);
-      store_cons(g.scr + S_FY * g.ps, g.ps, o, f);
+      store_cons(g.scr + S_FY * g.ps, g.ps, o, riemann<FLUX>(ul, ur, wl, wrt, b2l, g.eos));
     }
-    wl_prev = wln;
-    wa = wb;
-    wb = wc;
+    sh_store(sh, 3, tid, wln);
+    r0 = r1;
   }
 }
 
 // Resident blocks per SM the heavy kernels are compiled for (register caps of
 // 168 and 128 per thread): measured faster on B200 than the uncapped 255
 // registers and 2 blocks per SM despite the spills they cause.
-#ifndef ATHB_PREDICT_MINB
-#define ATHB_PREDICT_MINB 3
-#endif
-#ifndef ATHB_CORRECT_MINB
-#define ATHB_CORRECT_MINB 4
-#endif
+constexpr int kPredictMinBlocks = 3;
+constexpr int kCorrectMinBlocks = 4;
 
+// Block b of the predictor: the long role-Y column marches (ly rows each)
+// come first and the short role-X row segments (31 faces) last, so the
+// block scheduler ends the launch on small blocks instead of a tail of
+// marches.
 template <int FLUX>
 __device__ __forceinline__ void predict_block(const GridArgs& g, const PredictGeom& pg, int b) {
-  if (b < pg.nx_blocks) {
-    predict_x<FLUX>(g, b % pg.xseg, b / pg.xseg);
+  if (b < pg.ny_blocks) {
+    predict_y<FLUX>(g, pg, b);
   } else {
-    b -= pg.nx_blocks;
-    predict_y<FLUX>(g, b % pg.ycolblk, b / pg.ycolblk);
+    b -= pg.ny_blocks;
+    predict_x<FLUX>(g, b % pg.xseg, b / pg.xseg);
   }
 }
 
 template <int FLUX>
-static __global__ void __launch_bounds__(kThreads, ATHB_PREDICT_MINB) k_predict(GridArgs g, PredictGeom pg) {
+static __global__ void __launch_bounds__(kThreads, kPredictMinBlocks) k_predict(GridArgs g, PredictGeom pg) {
   if (g.st->done) return;
   predict_block<FLUX>(g, pg, blockIdx.x);
 }
@@ -427,7 +462,7 @@ __device__ __forceinline__ void correct_block(const GridArgs& g, const CorrectGe
 }
 
 template <int FLUX>
-static __global__ void __launch_bounds__(kThreads, ATHB_CORRECT_MINB) k_correct(GridArgs g, CorrectGeom cg) {
+static __global__ void __launch_bounds__(kThreads, kCorrectMinBlocks) k_correct(GridArgs g, CorrectGeom cg) {
   if (g.st->done) return;
   correct_block<FLUX>(g, cg, blockIdx.x);
 }

@@ -148,6 +148,14 @@ int athb_get_ly(const athb_ctx *ctx);
 /* The CUDA stream the context launches on (as a cudaStream_t).               */
 void *athb_stream(athb_ctx *ctx);
 
+/* Diagnostics of the resident state, computed on the GPU over the interior:
+ * out[0] mass, out[1] total energy, out[2] magnetic energy (sum of
+ * (B1c^2+B2c^2+B3c^2)/2 dV), out[3] sum of Bp2 = B1c^2+B2c^2 dV (the
+ * field-loop expression, src/field_loop.c:167-171), out[4] max |div B| from
+ * the face fields (constrained transport keeps it at round-off), out[5] max
+ * |J3| (src/field_loop.c:161-165).  Deterministic (fixed reduction order).  */
+int athb_diagnostics(athb_ctx *ctx, double out[6]);
+
 /* Pinned host memory for fast transfers. */
 void *athb_host_alloc(unsigned long long bytes);
 void athb_host_free(void *p);
@@ -217,6 +225,18 @@ int athb_batch_set_ly(athb_batch *b, int k, int ly);
 int athb_batch_commit(athb_batch *b);
 int athb_batch_set_grid(athb_batch *b, int blocks);
 int athb_batch_grid(const athb_batch *b);
+/* per-phase time, accumulated in ms_out[6]: predict, emf (half step),
+ * correct, emf (full step), update, ghost + finalize (persistent mode: block
+ * 0's view, each phase ending at its grid barrier; phased mode: between
+ * device time stamps after each phase).  enable: 1 start recording (resets),
+ * 0 stop, -1 leave as is; ms_out may be NULL.                              */
+int athb_batch_timing(athb_batch *b, int enable, double *ms_out);
+/* execution mode: one persistent cooperative launch per step (default), or
+ * one launch per phase with the hardware block scheduler; identical results */
+#define ATHB_BATCH_PERSISTENT 0
+#define ATHB_BATCH_PHASED 1
+int athb_batch_set_mode(athb_batch *b, int mode);
+int athb_batch_mode(const athb_batch *b);
 
 /* ---- allocation-free step ------------------------------------------------ */
 /* No counterpart in the reference.  One integrate_2d step (the cells

@@ -73,5 +73,25 @@ def test_batch_partial_runs_and_tuning_keep_results(tmp_path):
 def test_autotuner_returns_a_candidate():
     from athena_cuda_b200 import autotune
 
-    ly, times = autotune.tune_ly(24, 40, steps=2)
+    ly, times = autotune.tune_class(40, nx1=24, launches=1)
     assert ly in autotune.LY_CANDIDATES and ly in times and all(t > 0 for t in times.values())
+
+
+def test_phased_mode_matches_persistent():
+    """One launch per phase gives the same bits as the persistent kernel."""
+    items = _items()
+    want = Batch.from_problems(items)
+    want.run(10_000)
+    ref = [want.download(k) for k in range(want.n)]
+    want.close()
+    b = Batch.from_problems(items)
+    b.mode = Batch.PHASED
+    assert b.mode == Batch.PHASED
+    b.timing(1)
+    b.run(10_000)
+    assert all(v >= 0.0 for v in b.timing(0).values())
+    for k in range(b.n):
+        planes, dt, t, n = b.download(k)
+        assert refutil.mismatch_report(ref[k][0], planes, PLANES) == ""
+        assert (dt, t, n) == ref[k][1:]
+    b.close()
