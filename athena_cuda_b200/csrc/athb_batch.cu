@@ -50,13 +50,20 @@ struct BarrierState {
   unsigned int gen;
 };
 
-// Units of work: the 128-thread blocks of the single-grid kernels.  A work
-// item is a chunk of up to chunk_of(ph) consecutive units of one instance;
-// item w of phase ph is wmap[mbase[ph] + w].  Chunks amortise the per-item
-// cost (ticket, lookup, barriers) over several units; short units (EMF,
-// update, ghost fill) take longer chunks (chunk_of).
-__host__ __device__ constexpr int chunk_of(int ph) {
-  return ph == 0 ? 2 : ph == 2 ? 2 : ph == 1 || ph == 3 ? 8 : 4;
+// Units of work: the 128-thread blocks of the single-grid kernels.  The work
+// map has kSegs segments: the predictor's role-Y units of every active
+// instance, then its role-X units (so every long column march of the phase
+// is handed out before any short row segment and the phase ends on short
+// work), then one segment per later phase.  A work item is a chunk of up to
+// chunk_of(seg) consecutive units of one instance; item w of segment s is
+// wmap[mbase[s] + w].  Chunks amortise the per-item cost (ticket, lookup,
+// barriers) over several units; short units take longer chunks.
+constexpr int kSegs = kPhases + 1;
+enum Seg { kSegPredictY = 0, kSegPredictX, kSegEmfHalf, kSegCorrect, kSegEmfFull, kSegUpdate, kSegGhost };
+__host__ __device__ constexpr int seg_first(int ph) { return ph == 0 ? 0 : ph + 1; }  // phase -> first segment
+__host__ __device__ constexpr int chunk_of(int seg) {
+  return seg == kSegPredictY ? 1 : seg == kSegPredictX || seg == kSegCorrect ? 2
+       : seg == kSegEmfHalf || seg == kSegEmfFull ? 8 : 4;
 }
 
 struct __align__(16) WorkItem {
@@ -68,7 +75,7 @@ struct BatchDev {
   StepState* st;
   int* cur;
   unsigned int* ghost_left;
-  const int* mbase;     // kPhases + 1: start of each phase's items in wmap
+  const int* mbase;     // kSegs + 1: start of each segment's items in wmap
   const WorkItem* wmap;
   unsigned int* tick;   // kPhases work counters (dynamic item assignment)
   int n;
@@ -83,14 +90,17 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-__device__ __forceinline__ int item_count(const InstGeom& I, int ph) {
-  switch (ph) {
-  case 0: return I.pg.nx_blocks + I.pg.ny_blocks;
-  case 1: return (int)(((long long)(I.nx1 + 3) * (I.nx2 + 3) + kThreads - 1) / kThreads);
-  case 2: return I.cg.xb + I.cg.yb + I.cg.eb;
-  case 3: return (int)(((long long)(I.nx1 + 1) * (I.nx2 + 1) + kThreads - 1) / kThreads);
-  case 4: return (int)(((long long)I.nx1 * I.nx2 + kThreads - 1) / kThreads);
-  default: return (I.nframe + kThreads - 1) / kThreads;
+// Units of instance I in map segment seg.
+__host__ __device__ inline int item_count(const InstGeom& I, int seg) {
+  auto bf = [](long long n) { return (int)((n + kThreads - 1) / kThreads); };
+  switch (seg) {
+  case kSegPredictY: return I.pg.ny_blocks;
+  case kSegPredictX: return I.pg.nx_blocks;
+  case kSegEmfHalf: return bf((long long)(I.nx1 + 3) * (I.nx2 + 3));
+  case kSegCorrect: return I.cg.xb + I.cg.yb + I.cg.eb;
+  case kSegEmfFull: return bf((long long)(I.nx1 + 1) * (I.nx2 + 1));
+  case kSegUpdate: return bf((long long)I.nx1 * I.nx2);
+  default: return bf(I.nframe);
   }
 }
 
@@ -176,7 +186,7 @@ __device__ __forceinline__ void run_chunk(const BatchDev& B, int ph, int k, int 
       if (atomicSub(&B.ghost_left[k], (unsigned int)nb) == (unsigned int)nb) {
         // last ghost unit of instance k: end of its step
         __threadfence();
-        B.ghost_left[k] = (unsigned int)item_count(I, kPhases - 1);
+        B.ghost_left[k] = (unsigned int)item_count(I, kSegGhost);
         finalize_state(B.st[k], g.dx1, g.dx2, 1);
         B.cur[k] ^= 1;
         __threadfence();
@@ -201,8 +211,8 @@ __global__ void __launch_bounds__(kThreads, kBatchMinBlocks) k_batch_step(BatchD
   int k_prev = -1;  // instance held in s_I
   int cur_prev = -1;
   for (int ph = 0; ph < kPhases; ph++) {
-    const int base = B.mbase[ph];
-    const int total = B.mbase[ph + 1] - base;
+    const int base = B.mbase[seg_first(ph)];
+    const int total = B.mbase[seg_first(ph + 1)] - base;
     unsigned int* tick = B.tick + ph;
     if (threadIdx.x == 0) {
       // every block is past the previous phase: its counter is free again
@@ -259,8 +269,8 @@ template <int FLUX, int PH>
 __global__ void __launch_bounds__(kThreads, PhaseBlocks<PH>::value) k_batch_phase(BatchDev B) {
   __shared__ InstGeom s_I;
   __shared__ int s_k, s_b, s_nb, s_cur;
-  const int base = B.mbase[PH];
-  if ((int)blockIdx.x >= B.mbase[PH + 1] - base) return;
+  const int base = B.mbase[seg_first(PH)];
+  if ((int)blockIdx.x >= B.mbase[seg_first(PH + 1)] - base) return;
   if (threadIdx.x == 0) {
     const WorkItem it = B.wmap[base + blockIdx.x];
     s_k = it.id;
@@ -282,20 +292,22 @@ __global__ void k_stamp(unsigned long long* timing, int ph) {
   timing[kPhases] = now;
 }
 
-// wmap of the active instances: block (a, ph) writes the chunks of active
-// slot a in phase ph.
+// wmap of the active instances: block (a, seg) writes the chunks of active
+// slot a in segment seg.  Role-X units follow the role-Y units in the
+// predictor's block numbering (predict_block).
 __global__ void k_build_map(const InstGeom* inst, const int* off, const int* mbase, const int* ids, int n,
                             WorkItem* wmap) {
-  const int a = blockIdx.x, ph = blockIdx.y;
+  const int a = blockIdx.x, seg = blockIdx.y;
   if (a >= ids[n]) return;
-  const int* o = off + ph * (n + 1);
+  const int* o = off + seg * (n + 1);
   const int i0 = o[a], i1 = o[a + 1];
   const int id = ids[a];
-  const int units = item_count(inst[id], ph), r = chunk_of(ph);
-  WorkItem* m = wmap + mbase[ph];
+  const int units = item_count(inst[id], seg), r = chunk_of(seg);
+  const int first = seg == kSegPredictX ? inst[id].pg.ny_blocks : 0;
+  WorkItem* m = wmap + mbase[seg];
   for (int w = i0 + threadIdx.x; w < i1; w += blockDim.x) {
-    const int b0 = (w - i0) * r;
-    m[w] = WorkItem{id, b0, min(r, units - b0), 0};
+    const int u = (w - i0) * r;
+    m[w] = WorkItem{id, first + u, min(r, units - u), 0};
   }
 }
 
@@ -312,7 +324,7 @@ struct athb_batch {
   StepState* st = nullptr;
   int* cur = nullptr;
   unsigned int* ghost_left = nullptr;
-  int* off = nullptr;           // kPhases x (n+1) item prefix sums, then mbase (kPhases+1)
+  int* off = nullptr;           // kSegs x (n+1) item prefix sums, then mbase (kSegs+1)
   WorkItem* wmap = nullptr;     // item -> (instance, block), built on the device
   size_t wmap_cap = 0;
   unsigned int* tick = nullptr; // kPhases work counters
@@ -374,19 +386,9 @@ static InstGeom make_geom(const athb_config& c, int ly, double* state0, double* 
   return I;
 }
 
-static int host_items(const InstGeom& I, int ph) {
-  auto bf = [](long long n) { return (int)((n + kThreads - 1) / kThreads); };
-  switch (ph) {
-  case 0: return I.pg.nx_blocks + I.pg.ny_blocks;
-  case 1: return bf((long long)(I.nx1 + 3) * (I.nx2 + 3));
-  case 2: return I.cg.xb + I.cg.yb + I.cg.eb;
-  case 3: return bf((long long)(I.nx1 + 1) * (I.nx2 + 1));
-  case 4: return bf((long long)I.nx1 * I.nx2);
-  default: return bf(I.nframe);
-  }
+static int host_chunks(const InstGeom& I, int seg) {
+  return (item_count(I, seg) + chunk_of(seg) - 1) / chunk_of(seg);
 }
-
-static int host_chunks(const InstGeom& I, int ph) { return (host_items(I, ph) + chunk_of(ph) - 1) / chunk_of(ph); }
 
 static void release(athb_batch* b) {
   if (!b) return;
@@ -414,28 +416,27 @@ static void drop_graph(athb_batch* b) {
 // the tables through fixed device pointers, so it stays valid.
 static int upload_work(athb_batch* b) {
   const int n = b->n, na = (int)b->active.size();
-  std::vector<int> off((size_t)kPhases * (n + 1) + kPhases + 1, 0);
-  int* mbase = off.data() + (size_t)kPhases * (n + 1);
-  for (int ph = 0; ph < kPhases; ph++) {
+  std::vector<int> off((size_t)kSegs * (n + 1) + kSegs + 1, 0);
+  int* mbase = off.data() + (size_t)kSegs * (n + 1);
+  for (int seg = 0; seg < kSegs; seg++) {
     int acc = 0;
     for (int a = 0; a < na; a++) {
-      off[(size_t)ph * (n + 1) + a] = acc;
-      acc += host_chunks(b->geom[b->active[a]], ph);
+      off[(size_t)seg * (n + 1) + a] = acc;
+      acc += host_chunks(b->geom[b->active[a]], seg);
     }
-    off[(size_t)ph * (n + 1) + na] = acc;
-    mbase[ph + 1] = mbase[ph] + acc;
-    b->phase_total[ph] = acc;
+    off[(size_t)seg * (n + 1) + na] = acc;
+    mbase[seg + 1] = mbase[seg] + acc;
   }
-  if ((size_t)mbase[kPhases] > b->wmap_cap)
-    return athb_fail(ATHB_ERR_STATE, "work map capacity %zu < %d items", b->wmap_cap, mbase[kPhases]);
+  for (int ph = 0; ph < kPhases; ph++) b->phase_total[ph] = mbase[seg_first(ph + 1)] - mbase[seg_first(ph)];
+  if ((size_t)mbase[kSegs] > b->wmap_cap)
+    return athb_fail(ATHB_ERR_STATE, "work map capacity %zu < %d items", b->wmap_cap, mbase[kSegs]);
   std::vector<int> ids(n + 1, 0);
   for (int a = 0; a < na; a++) ids[a] = b->active[a];
   ids[n] = na;
-  if (b->mode == ATHB_BATCH_PHASED) drop_graph(b);  // its launches hold the per-phase grid sizes
   CUDA_TRY(cudaMemcpyAsync(b->off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
   CUDA_TRY(cudaMemcpyAsync(b->ids, ids.data(), ids.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
   if (na > 0) {
-    k_build_map<<<dim3(na, kPhases), kThreads, 0, b->stream>>>(b->dgeom, b->off, b->off + (size_t)kPhases * (n + 1),
+    k_build_map<<<dim3(na, kSegs), kThreads, 0, b->stream>>>(b->dgeom, b->off, b->off + (size_t)kSegs * (n + 1),
                                                                 b->ids, n, b->wmap);
     CUDA_TRY(cudaGetLastError());
   }
@@ -447,7 +448,7 @@ static int upload_work(athb_batch* b) {
 static int upload_tables(athb_batch* b) {
   const int n = b->n;
   std::vector<unsigned int> gl(n);
-  for (int k = 0; k < n; k++) gl[k] = (unsigned int)host_items(b->geom[k], kPhases - 1);
+  for (int k = 0; k < n; k++) gl[k] = (unsigned int)item_count(b->geom[k], kSegGhost);
   CUDA_TRY(cudaMemcpyAsync(b->dgeom, b->geom.data(), n * sizeof(InstGeom), cudaMemcpyHostToDevice, b->stream));
   CUDA_TRY(cudaMemcpyAsync(b->ghost_left, gl.data(), n * sizeof(unsigned int), cudaMemcpyHostToDevice, b->stream));
   if (b->active.empty()) {
@@ -456,7 +457,7 @@ static int upload_tables(athb_batch* b) {
   }
   size_t items = 0;  // every instance active: the largest map
   for (int k = 0; k < n; k++)
-    for (int ph = 0; ph < kPhases; ph++) items += (size_t)host_chunks(b->geom[k], ph);
+    for (int seg = 0; seg < kSegs; seg++) items += (size_t)host_chunks(b->geom[k], seg);
   if (items > b->wmap_cap) {
     drop_graph(b);
     cudaFree(b->wmap);
@@ -500,7 +501,7 @@ extern "C" int athb_batch_create(int n, const athb_config* cfgs, athb_batch** ou
   if (e == cudaSuccess) e = cudaMalloc(&b->st, n * sizeof(StepState));
   if (e == cudaSuccess) e = cudaMalloc(&b->cur, n * sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc(&b->ghost_left, n * sizeof(unsigned int));
-  if (e == cudaSuccess) e = cudaMalloc(&b->off, ((size_t)kPhases * (n + 1) + kPhases + 1) * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&b->off, ((size_t)kSegs * (n + 1) + kSegs + 1) * sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc(&b->tick, kPhases * sizeof(unsigned int));
   if (e == cudaSuccess) e = cudaMemsetAsync(b->tick, 0, kPhases * sizeof(unsigned int), b->stream);
   if (e == cudaSuccess) e = cudaMalloc(&b->ids, (size_t)(n + 1) * sizeof(int));
@@ -638,7 +639,7 @@ extern "C" int athb_batch_prepare(athb_batch* b) {
 static BatchDev batch_dev(const athb_batch* b) {
   BatchDev D;
   D.inst = b->dgeom; D.st = b->st; D.cur = b->cur; D.ghost_left = b->ghost_left;
-  D.mbase = b->off + (size_t)kPhases * (b->n + 1);
+  D.mbase = b->off + (size_t)kSegs * (b->n + 1);
   D.wmap = b->wmap;
   D.tick = b->tick;
   D.n = b->n; D.bar = b->bar; D.err = b->err;
@@ -687,13 +688,15 @@ static int launch_step(athb_batch* b) {
   return ATHB_OK;
 }
 
-// Launch nsteps steps (persistent: one cooperative launch each; phased: six
-// launches each; captured in a CUDA graph when the driver allows it) without
-// synchronising.
+// Launch nsteps steps without synchronising (persistent: one cooperative
+// launch each, captured in a CUDA graph when the driver allows it; phased:
+// six launches each).
 extern "C" int athb_batch_run_async(athb_batch* b, int nsteps) {
   if (!b || nsteps < 0) return athb_fail(ATHB_ERR_ARG, "bad arguments");
   CUDA_TRY(cudaSetDevice(b->device));
-  if (!b->graph && !b->graph_tried) {
+  // phased launches take their grid sizes from the active set, which changes
+  // as instances finish: launched directly (six launches a step)
+  if (b->mode == ATHB_BATCH_PERSISTENT && !b->graph && !b->graph_tried) {
     b->graph_tried = true;
     cudaGraph_t graph = nullptr;
     if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
@@ -707,7 +710,7 @@ extern "C" int athb_batch_run_async(athb_batch* b, int nsteps) {
     }
   }
   for (int s = 0; s < nsteps; s++) {
-    if (b->graph) CUDA_TRY(cudaGraphLaunch(b->graph, b->stream));
+    if (b->mode == ATHB_BATCH_PERSISTENT && b->graph) CUDA_TRY(cudaGraphLaunch(b->graph, b->stream));
     else { int rc = launch_step(b); if (rc) return rc; }
   }
   return ATHB_OK;

@@ -86,6 +86,22 @@ def dist_env():
     return ws, rank, local
 
 
+def max_over_ranks(x: float, ws: int, device) -> float:
+    """The slowest rank's device time (every rank takes part; all get it)."""
+    if ws == 1:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(ws: int, cells: int, ms_step: float) -> float:
+    """Whole-job zone-cycles/s of ws independent replicas of `cells` zones
+    whose slowest rank took ms_step per step."""
+    return ws * cells / (ms_step * 1e-3)
+
+
 def config_dict(a):
     return {"workload": f"field_loop {a.nx}x{a.ny}", "problem": "field_loop", "nx1": a.nx, "nx2": a.ny,
             "flux": "roe", "precision": "fp64", "cfl": 0.8, "l2": "inputs larger than L2 (372 MB state)",
@@ -262,13 +278,10 @@ def ours(a) -> None:
     ms = e0.elapsed_time(e1)
     st1 = g.status()
     assert st1["nstep"] - st0["nstep"] == a.steps and not st1["done"], "timed steps did not all run"
-    if ws > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, ws, torch.device("cuda", local))
     cells = a.nx * a.ny
     ms_step = ms / a.steps
-    value = ws * cells / (ms_step * 1e-3)
+    value = replica_value(ws, cells, ms_step)
 
     # per-kernel event timing (same stream, outside the graph)
     kms = (C.c_double * 7)()
