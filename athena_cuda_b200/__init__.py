@@ -100,6 +100,11 @@ def lib() -> C.CDLL:
             "athb_batch_timing": (I, [P, I, dp]),
             "athb_batch_set_mode": (I, [P, I]),
             "athb_batch_mode": (I, [P]),
+            "athb_batch_generate": (I, [P, I, C.c_char_p, P]),
+            "athb_generate": (I, [P, C.c_char_p, P]),
+            "athb_set_pause": (I, [P, D, I]),
+            "athb_dump_bin": (I, [P, C.c_char_p]),
+            "athb_dump_tab": (I, [P, C.c_char_p, C.c_char_p]),
             "athb_profile_steps": (I, [P, I, dp]),
             "athb_fp64_peak": (I, [I, dp]),
             "athb_set_ly": (I, [P, I]),
@@ -121,6 +126,10 @@ def _check(rc: int) -> None:
 
 def _dp(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+# problem generators with a device form (athb_generate / athb_batch_generate)
+DEVICE_PROBLEMS = ("blast", "field_loop")
 
 
 class Params:
@@ -246,7 +255,8 @@ class Grid:
     def status(self) -> dict:
         t, dt, n, done = C.c_double(), C.c_double(), C.c_int(), C.c_int()
         _check(lib().athb_status(self._h, C.byref(t), C.byref(dt), C.byref(n), C.byref(done)))
-        return {"time": t.value, "dt": dt.value, "nstep": n.value, "done": bool(done.value)}
+        return {"time": t.value, "dt": dt.value, "nstep": n.value, "done": done.value == 1,
+                "paused": done.value == 2}
 
     @property
     def stream(self) -> int:
@@ -276,6 +286,23 @@ class Grid:
         err = np.zeros(9)
         _check(lib().athb_cpaw2d_errors(self._h, _dp(err)))
         return err
+
+    def generate(self, name: str, params: "Params") -> None:
+        """Replace the state with problem `name`'s initial condition (clock
+        reset, no ghost fill); blast and field_loop are formed on the GPU."""
+        _check(lib().athb_generate(self._h, name.encode(), params._h))
+
+    def set_pause(self, tpause: float, on: bool = True) -> None:
+        """Stop the device loop at the first step starting at time >= tpause."""
+        _check(lib().athb_set_pause(self._h, tpause, int(on)))
+
+    def dump_bin(self, path) -> None:
+        """The reference's binary dump of the current state (src/dump_binary.c)."""
+        _check(lib().athb_dump_bin(self._h, str(path).encode()))
+
+    def dump_tab(self, path, dat_fmt: str | None = None) -> None:
+        """The reference's table dump of the current state (src/dump_tab.c)."""
+        _check(lib().athb_dump_tab(self._h, str(path).encode(), dat_fmt.encode() if dat_fmt else None))
 
     def close(self) -> None:
         if self._h:
@@ -325,9 +352,16 @@ class Batch:
         cfgs = [p.config() for p in params]
         b = cls(cfgs)
         for k, ((name, _), p) in enumerate(zip(items, params)):
-            b.upload(k, problem_state(name, p))
+            if name in DEVICE_PROBLEMS:
+                b.generate(k, name, p)  # formed on the GPU
+            else:
+                b.upload(k, problem_state(name, p))
         b.prepare()
         return b
+
+    def generate(self, k: int, name: str, params: "Params") -> None:
+        """Instance k's initial condition formed on the GPU (DEVICE_PROBLEMS)."""
+        _check(lib().athb_batch_generate(self._h, k, name.encode(), params._h))
 
     def upload(self, k: int, planes: np.ndarray, dt=0.0, time=0.0, nstep=0) -> None:
         planes = np.ascontiguousarray(planes, dtype=np.float64)

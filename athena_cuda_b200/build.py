@@ -20,6 +20,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OBJ = PKG / "_build"
 LIB = PKG / "libathena_b200.so"
+EXE = PKG / "athena_b200"
 
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 CUDA_HOME = Path(NVCC).resolve().parent.parent
@@ -31,7 +32,8 @@ NVCC_FLAGS = ARCH + [
 CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", f"-I{ROOT / 'include'}",
              f"-I{CUDA_HOME / 'include'}"]
 
-CU_SOURCES = ["athb_core.cu", "athb_dropin.cu", "athb_batch.cu", "athb_noalloc.cu"]
+CU_SOURCES = ["athb_core.cu", "athb_dropin.cu", "athb_batch.cu", "athb_noalloc.cu", "athb_output.cu",
+              "athb_problems_dev.cu"]
 CPP_SOURCES = ["athinput.cpp", "problems.cpp"]
 HEADERS = ["mhd_physics.cuh", "step_types.cuh", "step_kernels.cuh", "athb_internal.h"]
 
@@ -77,6 +79,10 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False,
         objs.append(o)
     if force or _stale(lib, objs):
         _run([NVCC, *ARCH, "-shared", "-o", str(lib), *map(str, objs), "-lcudart"], verbose)
+    if lib == LIB:  # the command-line driver, next to the library it links
+        if force or _stale(EXE, [CSRC / "athena_main.cpp", lib] + hdrs):
+            _run(["g++", *CXX_FLAGS, "-o", str(EXE), str(CSRC / "athena_main.cpp"), f"-L{PKG}", "-lathena_b200",
+                  "-Wl,-rpath,$ORIGIN"], verbose)
     return lib
 
 

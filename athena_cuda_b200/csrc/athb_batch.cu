@@ -571,25 +571,61 @@ extern "C" int athb_batch_set_grid(athb_batch* b, int blocks) {
   return ATHB_OK;
 }
 
+// Instance k's clock (dt as the reference Grid holds it; the next step takes
+// it after the tlim clamp, src/main.c:230-232).
+static int set_inst_clock(athb_batch* b, int k, double dt, double time, int nstep) {
+  const InstGeom& I = b->geom[k];
+  const athb_config& c = b->cfg[k];
+  StepState h{};
+  h.time = time; h.tlim = c.tlim; h.cour_no = c.cour_no; h.nstep = nstep; h.nlim = c.nlim;
+  h.done = !((time < c.tlim) && (c.nlim < 0 || nstep < c.nlim));
+  h.dt_new = dt;
+  h.dt = (!h.done && (h.tlim - time) < dt) ? (h.tlim - time) : dt;
+  h.dtodx1 = h.dt / I.g.dx1; h.dtodx2 = h.dt / I.g.dx2;
+  h.hdtodx1 = 0.5 * h.dtodx1; h.hdtodx2 = 0.5 * h.dtodx2; h.hdt = 0.5 * h.dt;
+  CUDA_TRY(cudaMemcpyAsync(b->st + k, &h, sizeof h, cudaMemcpyHostToDevice, b->stream));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  return ATHB_OK;
+}
+
+// The buffer holding instance k's current state.
+static int inst_state(athb_batch* b, int k, double** state) {
+  const InstGeom& I = b->geom[k];
+  int cur = 0;
+  CUDA_TRY(cudaMemcpy(&cur, b->cur + k, sizeof(int), cudaMemcpyDeviceToHost));
+  *state = cur ? I.g.out : const_cast<double*>(I.g.in);
+  return ATHB_OK;
+}
+
 // Load instance k's state (host SoA planes, as athb_upload) and its clock.
 extern "C" int athb_batch_upload(athb_batch* b, int k, const double* planes, double dt, double time, int nstep) {
   if (!b || k < 0 || k >= b->n || !planes) return athb_fail(ATHB_ERR_ARG, "bad arguments");
   CUDA_TRY(cudaSetDevice(b->device));
   const InstGeom& I = b->geom[k];
-  int cur = 0;
-  CUDA_TRY(cudaMemcpy(&cur, b->cur + k, sizeof(int), cudaMemcpyDeviceToHost));
-  double* dst = cur ? I.g.out : const_cast<double*>(I.g.in);
+  double* dst = nullptr;
+  int rc = inst_state(b, k, &dst);
+  if (rc) return rc;
   CUDA_TRY(cudaMemcpy2DAsync(dst, sizeof(double) * I.g.pitch, planes, sizeof(double) * I.sx,
                              sizeof(double) * I.sx, (size_t)I.sy * NSTATE, cudaMemcpyHostToDevice, b->stream));
-  StepState h{};
-  const athb_config& c = b->cfg[k];
-  h.dt = dt; h.time = time; h.tlim = c.tlim; h.cour_no = c.cour_no; h.nstep = nstep; h.nlim = c.nlim;
-  h.done = !((time < c.tlim) && (c.nlim < 0 || nstep < c.nlim));
-  h.dtodx1 = dt / I.g.dx1; h.dtodx2 = dt / I.g.dx2;
-  h.hdtodx1 = 0.5 * h.dtodx1; h.hdtodx2 = 0.5 * h.dtodx2; h.hdt = 0.5 * dt;
-  CUDA_TRY(cudaMemcpyAsync(b->st + k, &h, sizeof h, cudaMemcpyHostToDevice, b->stream));
-  CUDA_TRY(cudaStreamSynchronize(b->stream));
-  return ATHB_OK;
+  return set_inst_clock(b, k, dt, time, nstep);
+}
+
+// Instance k's initial condition formed on the GPU (built-in "blast" and
+// "field_loop", as athb_generate); clock reset.  Other problems: upload.
+extern "C" int athb_batch_generate(athb_batch* b, int k, const char* name, const athb_params* p) {
+  if (!b || k < 0 || k >= b->n || !name || !p) return athb_fail(ATHB_ERR_ARG, "bad arguments");
+  CUDA_TRY(cudaSetDevice(b->device));
+  const int kind = athb_builtin_problem(name);
+  if (kind != kProblemBlast && kind != kProblemFieldLoop)
+    return athb_fail(ATHB_ERR_NOTFOUND, "problem \"%s\" has no device generator (use athb_batch_upload)", name);
+  const InstGeom& I = b->geom[k];
+  double* dst = nullptr;
+  int rc = inst_state(b, k, &dst);
+  if (rc) return rc;
+  rc = athb_generate_device_into(kind, p, dst, I.g.scr + (size_t)S_EMF * I.g.ps, I.g.ps, I.g.pitch, b->cfg[k],
+                                 b->stream);
+  if (rc) return rc;
+  return set_inst_clock(b, k, 0.0, 0.0, 0);
 }
 
 extern "C" int athb_batch_download(athb_batch* b, int k, double* planes, double* dt, double* time, int* nstep) {
@@ -606,7 +642,7 @@ extern "C" int athb_batch_download(athb_batch* b, int k, double* planes, double*
   StepState h;
   CUDA_TRY(cudaMemcpyAsync(&h, b->st + k, sizeof h, cudaMemcpyDeviceToHost, b->stream));
   CUDA_TRY(cudaStreamSynchronize(b->stream));
-  if (dt) *dt = h.dt;
+  if (dt) *dt = h.dt_new;
   if (time) *time = h.time;
   if (nstep) *nstep = h.nstep;
   return ATHB_OK;

@@ -184,18 +184,21 @@ extern "C" void athb_host_free(void* p) { if (p) cudaFreeHost(p); }
 // ---------------------------------------------------------------------------
 int athb_set_clock(athb_ctx* c, double dt, double time, int nstep) {
   StepState h{};
-  h.dt = dt;
   h.time = time;
   h.tlim = c->cfg.tlim;
   h.cour_no = c->cfg.cour_no;
   h.nstep = nstep;
   h.nlim = c->cfg.nlim;
   h.done = !((time < c->cfg.tlim) && (c->cfg.nlim < 0 || nstep < c->cfg.nlim));
-  h.dtodx1 = dt / c->dx1;
-  h.dtodx2 = dt / c->dx2;
+  // dt as the reference Grid holds it; the next step takes it after the tlim
+  // clamp (src/main.c:230-232)
+  h.dt_new = dt;
+  h.dt = (!h.done && (h.tlim - time) < dt) ? (h.tlim - time) : dt;
+  h.dtodx1 = h.dt / c->dx1;
+  h.dtodx2 = h.dt / c->dx2;
   h.hdtodx1 = 0.5 * h.dtodx1;
   h.hdtodx2 = 0.5 * h.dtodx2;
-  h.hdt = 0.5 * dt;
+  h.hdt = 0.5 * h.dt;
   CUDA_TRY(cudaMemcpyAsync(c->st, &h, sizeof h, cudaMemcpyHostToDevice, c->stream));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   return ATHB_OK;
@@ -226,7 +229,7 @@ extern "C" int athb_download(athb_ctx* c, double* planes, double* dt, double* ti
   StepState h;
   int rc = athb_read_clock(c, &h);
   if (rc) return rc;
-  if (dt) *dt = h.dt;
+  if (dt) *dt = h.dt_new;
   if (time) *time = h.time;
   if (nstep) *nstep = h.nstep;
   return ATHB_OK;
@@ -400,7 +403,7 @@ extern "C" int athb_status(athb_ctx* c, double* time, double* dt, int* nstep, in
   int rc = athb_read_clock(c, &h);
   if (rc) return rc;
   if (time) *time = h.time;
-  if (dt) *dt = h.dt;
+  if (dt) *dt = h.dt_new;
   if (nstep) *nstep = h.nstep;
   if (done) *done = h.done;
   if (h.flags & kErrNonFinite)
@@ -419,7 +422,8 @@ extern "C" int athb_run(athb_ctx* c, int nsteps, int* steps_done) {
   const int start = h.nstep;
   long long launched = 0;
   while (!h.done && launched < nsteps) {
-    double est = (h.tlim - h.time) / h.dt;
+    const double tend = h.has_pause ? std::min(h.tlim, h.tpause) : h.tlim;
+    double est = (tend - h.time) / h.dt;
     long long want = est < 1.0 ? 1 : (long long)std::ceil(est);
     if (h.nlim >= 0) want = std::min<long long>(want, std::max(1, h.nlim - h.nstep));
     want = std::min<long long>(want, nsteps - launched);
@@ -434,6 +438,17 @@ extern "C" int athb_run(athb_ctx* c, int nsteps, int* steps_done) {
   rc = athb_status(c, nullptr, nullptr, &nstep, nullptr);
   if (steps_done) *steps_done = nstep - start;
   return rc;
+}
+
+// Pause the loop at the first step that starts at time >= tpause (on != 0),
+// or run freely (on == 0).  athb_status then reports done = 2.
+extern "C" int athb_set_pause(athb_ctx* c, double tpause, int on) {
+  if (!c) return athb_fail(ATHB_ERR_ARG, "null context");
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  k_set_pause<<<1, 1, 0, c->stream>>>(c->st, tpause, on ? 1 : 0);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return ATHB_OK;
 }
 
 extern "C" int athb_set_bvals(athb_ctx* c) {

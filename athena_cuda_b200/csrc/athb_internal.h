@@ -41,3 +41,11 @@ int athb_launch_ghost(athb_ctx* c, int buf);
 int athb_launch_ghost_phase(athb_ctx* c, int buf, int mode, int sides);
 int athb_launch_cfl(athb_ctx* c, int buf);
 int athb_launch_set_dt(athb_ctx* c, double dt);
+int athb_read_clock(athb_ctx* c, athb::StepState* h);
+
+// problem generators (problems.cpp, athb_problems_dev.cu)
+enum { kProblemNone = 0, kProblemBlast, kProblemFieldLoop, kProblemCpaw2d };
+int athb_builtin_problem(const char* name);  // kind of the registered generator, if built in
+int athb_generate_host(athb_ctx* c, const char* name, const athb_params* p);
+int athb_generate_device_into(int kind, const athb_params* p, double* state, double* az, long long ps, int pitch,
+                              const athb_config& cfg, cudaStream_t stream);

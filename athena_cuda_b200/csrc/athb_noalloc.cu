@@ -50,7 +50,9 @@ __global__ void k_noalloc_begin(StepState* st, double dt, double dx1, double dx2
   StepState s;
   s.time = 0.0; s.tlim = 0.0; s.cour_no = 0.0;
   s.nstep = 0; s.nlim = -1; s.done = 0; s.flags = 0; s.max_dti_bits = 0ull;
+  s.tpause = 0.0; s.has_pause = 0;
   s.dt = dt;
+  s.dt_new = dt;
   s.dtodx1 = dt / dx1;
   s.dtodx2 = dt / dx2;
   s.hdtodx1 = 0.5 * s.dtodx1;

@@ -142,7 +142,7 @@ extern "C" int athb_params_geti(const athb_params* p, const char* block, const c
   return ATHB_OK;
 }
 
-const char* athb_params_gets(const athb_params* p, const char* block, const char* name) {
+extern "C" const char* athb_params_gets(const athb_params* p, const char* block, const char* name) {
   const std::string* s = p ? p->find(block, name) : nullptr;
   return s ? s->c_str() : nullptr;
 }

@@ -1,7 +1,8 @@
 // problems.cpp -- problem-generator hooks (initial conditions) and the cpaw2d
-// error diagnostic.  Initial conditions are set once, on the host, with the
-// reference's libm calls (sqrt/sin/cos/atan), so the state uploaded to the GPU
-// is bit-identical to the reference's; everything after that runs on the GPU.
+// error diagnostic.  The host generators use the reference's libm calls
+// (sqrt/sin/cos/atan), so a state they produce is bit-identical to the
+// reference's; athb_generate forms blast and field-loop states on the GPU
+// instead (athb_problems_dev.cu) and uses these for the rest.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -233,6 +234,36 @@ extern "C" int athb_problem_generate(const char* name, const athb_grid_info* g, 
   return ATHB_OK;
 }
 
+// Kind of the generator registered under `name` when it is a built-in one
+// (a user registration under the same name replaces it).
+int athb_builtin_problem(const char* name) {
+  auto it = registry().find(name ? name : "");
+  if (it == registry().end()) return kProblemNone;
+  if (it->second.fn == problem_blast) return kProblemBlast;
+  if (it->second.fn == problem_field_loop) return kProblemFieldLoop;
+  if (it->second.fn == problem_cpaw2d) return kProblemCpaw2d;
+  return kProblemNone;
+}
+
+// The host path of athb_generate: run the registered generator on a host
+// array and upload it (clock reset to dt = time = nstep = 0).
+int athb_generate_host(athb_ctx* c, const char* name, const athb_params* p) {
+  athb_grid_info gi;
+  int rc = athb_grid_info_of(c, &gi);
+  if (rc) return rc;
+  std::vector<double> planes((size_t)ATHB_NPLANES * gi.sx * gi.sy, 0.0);
+  rc = athb_problem_generate(name, &gi, p, planes.data());
+  if (rc) return rc;
+  if (athb_builtin_problem(name) == kProblemCpaw2d) {
+    // keep the initial cell-centred state: src/cpaw2d.c:160-180 (Soln)
+    const size_t n = (size_t)8 * gi.sx * gi.sy;
+    delete[] c->cpaw_soln;
+    c->cpaw_soln = new double[n];
+    memcpy(c->cpaw_soln, planes.data(), n * sizeof(double));
+  }
+  return athb_upload(c, planes.data(), 0.0, 0.0, 0);
+}
+
 extern "C" int athb_create_from_athinput(const char* path, int noverride, const char* const* overrides,
                                          const char* problem, athb_ctx** out) {
   if (!out) return athb_fail(ATHB_ERR_ARG, "null output pointer");
@@ -245,22 +276,9 @@ extern "C" int athb_create_from_athinput(const char* path, int noverride, const 
   if (rc == ATHB_OK) rc = athb_config_from_params(p, &cfg);
   athb_ctx* c = nullptr;
   if (rc == ATHB_OK) rc = athb_create(&cfg, &c);
-  std::vector<double> planes;
-  athb_grid_info gi;
-  if (rc == ATHB_OK) {
-    athb_grid_info_of(c, &gi);
-    planes.assign((size_t)ATHB_NPLANES * gi.sx * gi.sy, 0.0);
-    rc = athb_problem_generate(problem, &gi, p, planes.data());
-  }
-  athb_params_close(p);
-  if (rc == ATHB_OK && !strcmp(problem, "cpaw2d")) {
-    // keep the initial cell-centred state: src/cpaw2d.c:160-180 (Soln)
-    const size_t n = (size_t)8 * gi.sx * gi.sy;
-    c->cpaw_soln = new double[n];
-    memcpy(c->cpaw_soln, planes.data(), n * sizeof(double));
-  }
   // src/main.c:124-149: problem -> set_bvals -> new_dt
-  if (rc == ATHB_OK) rc = athb_upload(c, planes.data(), 0.0, 0.0, 0);
+  if (rc == ATHB_OK) rc = athb_generate(c, problem, p);
+  athb_params_close(p);
   if (rc == ATHB_OK) rc = athb_set_bvals(c);
   if (rc == ATHB_OK) rc = athb_new_dt(c, nullptr);
   if (rc) { athb_destroy(c); return rc; }

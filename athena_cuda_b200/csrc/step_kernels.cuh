@@ -618,10 +618,21 @@ __device__ __forceinline__ void finalize_state(StepState& st, double dx1, double
   st.max_dti_bits = 0ull;
   if (st.nstep == 0) st.dt = st.cour_no / max_dti;
   else st.dt = rmin(2.0 * st.dt, st.cour_no / max_dti);
+  st.dt_new = st.dt;
   const bool more = (st.time < st.tlim) && (st.nlim < 0 || st.nstep < st.nlim);
   st.done = more ? 0 : 1;
   if (more && (st.tlim - st.time) < st.dt) st.dt = (st.tlim - st.time);
+  if (more && st.has_pause && st.time >= st.tpause) st.done = 2;  // a host output is due first
   set_step_coeffs(st, dx1, dx2);
+}
+
+// Set (on != 0) or clear the pause time; a grid that has not ended runs or
+// stays paused according to it.
+static __global__ void k_set_pause(StepState* stp, double tpause, int on) {
+  StepState& st = *stp;
+  st.has_pause = on;
+  st.tpause = tpause;
+  if (st.done != 1) st.done = (on && st.time >= tpause) ? 2 : 0;
 }
 
 static __global__ void k_finalize(StepState* stp, double dx1, double dx2, int mode) {
@@ -631,6 +642,7 @@ static __global__ void k_finalize(StepState* stp, double dx1, double dx2, int mo
 // Set dt from the host value without any rule (drop-in integrate_2d path).
 static __global__ void k_set_dt(StepState* stp, double dt, double dx1, double dx2) {
   stp->dt = dt;
+  stp->dt_new = dt;
   stp->done = 0;
   set_step_coeffs(*stp, dx1, dx2);
 }

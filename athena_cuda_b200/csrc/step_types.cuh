@@ -23,16 +23,21 @@ enum BcKind { BC_REFLECT = 1, BC_OUTFLOW = 2, BC_PERIODIC = 4 };
 
 // Device-resident time-stepping state of one grid.
 struct StepState {
-  double dt;        // dt as the reference Grid holds it
+  double dt;        // dt of the next step (after the tlim clamp of src/main.c:230-232)
+  double dt_new;    // dt as the reference Grid holds it between iterations:
+                    // new_dt's value, before the next iteration's tlim clamp
   double time;
   double tlim;
   double cour_no;
   // derived from the dt the next step uses (src/__integrate_2d__.c:102-110)
   double dtodx1, dtodx2, hdtodx1, hdtodx2, hdt;
+  double tpause;    // with has_pause: stop stepping once time >= tpause
   int nstep;
   int nlim;         // < 0: no cycle limit
-  int done;         // 1 once time >= tlim or nstep >= nlim: steps become no-ops
+  int done;         // 1 once time >= tlim or nstep >= nlim (ended), 2 paused at
+                    // tpause; either way steps are no-ops
   int flags;        // error bits, see kErr*
+  int has_pause;
   unsigned long long max_dti_bits;  // running max of 1/dt (positive doubles
                                     // order like their bit patterns)
 };

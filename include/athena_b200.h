@@ -89,6 +89,7 @@ void new_dt(athb_Grid *pG);
 #define ATHB_ERR_PARSE 4    /* athinput file or parameter error              */
 #define ATHB_ERR_NOMEM 5    /* allocation failure                            */
 #define ATHB_ERR_NOTFOUND 6 /* unknown problem generator / parameter         */
+#define ATHB_ERR_IO 7       /* file open / write error                       */
 
 #define ATHB_FLUX_ROE 0     /* reference default (flux_roe, HLLE fallback)   */
 #define ATHB_FLUX_HLLE 1    /* flux_hlle everywhere                          */
@@ -133,6 +134,9 @@ int athb_new_dt(athb_ctx *ctx, double *dt);
 /* Run up to nsteps iterations of the reference main loop (clamp, step,
  * time += dt, new_dt, set_bvals) on the device; stops early at tlim/nlim.   */
 int athb_run(athb_ctx *ctx, int nsteps, int *steps_done);
+/* time, dt as the reference Grid holds it between iterations (new_dt's value;
+ * the next step takes it after the tlim clamp, src/main.c:230-232), nstep,
+ * done (0 running, 1 ended at tlim/nlim, 2 paused, see athb_set_pause).      */
 int athb_status(athb_ctx *ctx, double *time, double *dt, int *nstep, int *done);
 int athb_synchronize(athb_ctx *ctx);
 /* Launch-only variant of athb_run for timing (no synchronisation).          */
@@ -147,6 +151,21 @@ int athb_set_ly(athb_ctx *ctx, int ly);
 int athb_get_ly(const athb_ctx *ctx);
 /* The CUDA stream the context launches on (as a cudaStream_t).               */
 void *athb_stream(athb_ctx *ctx);
+/* Pause the device loop at the first iteration that starts at time >= tpause
+ * (on != 0; athb_run then returns there and athb_status reports done = 2),
+ * or run freely (on = 0).  For host work due at a given simulation time,
+ * such as the reference's data_output (src/main.c:239), without a host
+ * round trip per step.                                                      */
+int athb_set_pause(athb_ctx *ctx, double tpause, int on);
+
+/* Data dumps of the resident state, byte-identical to the reference's:
+ * athb_dump_bin writes dump_binary's file (src/dump_binary.c:25-134; the
+ * interior is converted to float on the GPU), athb_dump_tab dump_tab's
+ * (src/dump_tab.c:28-235; the middle row j = (js+je)/2; dat_fmt NULL for
+ * the default " %12.8e").  The caller forms the file name
+ * (src/ath_files.c:31-65: <problem_id>.<4-digit number>.<bin|tab>).        */
+int athb_dump_bin(athb_ctx *ctx, const char *path);
+int athb_dump_tab(athb_ctx *ctx, const char *path, const char *dat_fmt);
 
 /* Diagnostics of the resident state, computed on the GPU over the interior:
  * out[0] mass, out[1] total energy, out[2] magnetic energy (sum of
@@ -169,6 +188,8 @@ int athb_params_from_string(const char *text, athb_params **out);
 int athb_params_override(athb_params *p, const char *arg);
 int athb_params_getd(const athb_params *p, const char *block, const char *name, double *v);
 int athb_params_geti(const athb_params *p, const char *block, const char *name, int *v);
+/* the value text, or NULL when block/name does not exist (src/par.c:par_exist) */
+const char *athb_params_gets(const athb_params *p, const char *block, const char *name);
 void athb_params_close(athb_params *p);
 /* config from the <grid>, <time> and <problem> blocks */
 int athb_config_from_params(const athb_params *p, athb_config *cfg);
@@ -190,9 +211,17 @@ int athb_grid_info_of(const athb_ctx *ctx, athb_grid_info *g);
 int athb_problem_generate(const char *name, const athb_grid_info *g, const athb_params *p,
                           double *planes);
 
+/* Replace the resident state with problem `name`'s initial condition (clock
+ * reset to dt = time = nstep = 0; no set_bvals).  The built-in "blast" and
+ * "field_loop" generators run on the GPU in the state buffer (no host array,
+ * no upload; per cell they need only + - * / and sqrt, so the state is
+ * bit-identical to the host generators'); "cpaw2d" (libm sin/cos per cell)
+ * and registered generators run on the host and are uploaded.               */
+int athb_generate(athb_ctx *ctx, const char *name, const athb_params *p);
+
 /* Parse an athinput file (+ overrides), create the context, run the problem
- * generator, set_bvals and the first new_dt: the state src/main.c:75-149
- * holds on entry to its main loop.                                          */
+ * generator (athb_generate), set_bvals and the first new_dt: the state
+ * src/main.c:75-149 holds on entry to its main loop.                        */
 int athb_create_from_athinput(const char *path, int noverride, const char *const *overrides,
                               const char *problem, athb_ctx **out);
 
@@ -212,6 +241,9 @@ int athb_batch_size(const athb_batch *b);
 /* instance state in the athb_upload layout, and its clock                   */
 int athb_batch_upload(athb_batch *b, int k, const double *planes, double dt, double time, int nstep);
 int athb_batch_download(athb_batch *b, int k, double *planes, double *dt, double *time, int *nstep);
+/* instance k's initial condition formed on the GPU (built-in "blast" and
+ * "field_loop" only, see athb_generate), clock reset                        */
+int athb_batch_generate(athb_batch *b, int k, const char *name, const athb_params *p);
 /* set_bvals and the first new_dt of every instance (src/main.c:139-149)      */
 int athb_batch_prepare(athb_batch *b);
 /* steps until every instance is done or max_steps launches                  */

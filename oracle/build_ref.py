@@ -15,6 +15,11 @@ Builds, per problem generator and flux:
   reference's host-side files (``init_grid.c``, ``par.c``, the problem file)
   linked against ``libathena_b200.so`` instead of the reference's integrator,
   boundary and dt sources -- the drop-in test (only when the library exists).
+* ``athmain_{blast,field_loop,cpaw2d}``: the reference's own ``src/main.c``
+  with its output code (``output.c``, ``dump_binary.c``, ``dump_tab.c`` ...),
+  the program whose output files the command-line driver must reproduce;
+  ``oracle/ref_stubs.c`` supplies ``dt_destruct``, which ``main.c`` calls and
+  only the reference's CUDA engine defines.
 
 Flags: ``-O2 -ffp-contract=off`` (no FMA contraction, so every ``+ - * /`` and
 ``sqrt`` is one IEEE-754 binary64 operation).  The reference's own Debug flags
@@ -50,6 +55,11 @@ PROBLEMS = {
     "cpaw2d": ("cpaw2d.c", ["-DCPAW2D"]),
     "file": (None, ["-DHARNESS_FILE_PROBLEM"]),
 }
+# The reference's main program and its output path (athmain_*).
+MAIN_EXTRA = [
+    "main.c", "ath_files.c", "debug_tools_cuda.c", "dump_binary.c", "dump_tab.c", "output.c",
+    "output_ppm.c", "output_tab.c", "show_config.c", "utils_cu.c",
+]
 # ath_array.c:calloc_*_array_cu call cudaMalloc (never reached on this path),
 # so the CUDA runtime is linked only to resolve those symbols.
 LDCUDA = ["-L/usr/local/cuda/lib64", "-Wl,-rpath,/usr/local/cuda/lib64", "-lcudart"]
@@ -97,6 +107,14 @@ def build(ref_root: Path = DEFAULT_REF, force: bool = False, lib: Path | None = 
         for flux, iobj in integ.items():
             exe = OUT / f"athref_{prob}_{flux}"
             deps = [harness, iobj, *core, *pobj]
+            if force or not _newer(exe, deps):
+                _run(["gcc", "-o", str(exe), *map(str, deps), *LDCUDA, "-lm"])
+            built.append(exe)
+        if pfile is not None:
+            mobj = [_cc(src / f, obj / f"main_{prob}_{f[:-2]}.o", pdefs, inc, force) for f in MAIN_EXTRA]
+            stub = _cc(HERE / "ref_stubs.c", obj / "ref_stubs.o", [], inc, force)
+            exe = OUT / f"athmain_{prob}"
+            deps = [*mobj, stub, integ["roe"], *core, *pobj]
             if force or not _newer(exe, deps):
                 _run(["gcc", "-o", str(exe), *map(str, deps), *LDCUDA, "-lm"])
             built.append(exe)
