@@ -618,3 +618,109 @@ extern "C" int athb_diagnostics(athb_ctx* c, double out[6]) {
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   return ATHB_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Pieces of a main-loop iteration for callers that split a grid over several
+// contexts (a slab decomposition along x2, one context per GPU): the step of
+// the local interior, the local and the imposed CFL maximum, the ghost fill
+// by direction and side, and row transfers for the exchange of the
+// inter-slab ghost rows.
+// ---------------------------------------------------------------------------
+namespace {
+__global__ void k_set_max_dti(StepState* st, unsigned long long bits) { st->max_dti_bits = bits; }
+}  // namespace
+
+// Cell sizes and origin of the local grid (a slab takes the global grid's dx
+// exactly, which (x2max - x2min) / Nx2 of the slab need not reproduce).
+extern "C" int athb_set_geometry(athb_ctx* c, double dx1, double dx2, double x1_0, double x2_0) {
+  if (!c || !(dx1 > 0.0) || !(dx2 > 0.0)) return athb_fail(ATHB_ERR_ARG, "bad arguments");
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->dx1 = dx1; c->dx2 = dx2; c->x1_0 = x1_0; c->x2_0 = x2_0;
+  drop_graphs(c);
+  StepState h;
+  int rc = athb_read_clock(c, &h);
+  if (rc) return rc;
+  return athb_set_clock(c, h.dt_new, h.time, h.nstep);  // dt/dx factors of the new dx
+}
+
+// integrate_2d of the local interior (src/__integrate_2d__.c:100-537) into
+// the other buffer, 1/dt of every updated cell folded into the context's
+// running maximum; no time advance, no new dt, no ghost fill (see
+// athb_finish_step).
+extern "C" int athb_integrate_local(athb_ctx* c) {
+  if (!c) return athb_fail(ATHB_ERR_ARG, "null context");
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  return athb_launch_integrate(c, c->cur);
+}
+
+// 1/dt of the resident interior folded into the running maximum (new_dt
+// before the loop, src/main.c:149).
+extern "C" int athb_cfl_local(athb_ctx* c) {
+  if (!c) return athb_fail(ATHB_ERR_ARG, "null context");
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  return athb_launch_cfl(c, c->cur);
+}
+
+// The running maximum of 1/dt as the bits of a positive double (which order
+// like the doubles): the value to reduce with a max across contexts.
+extern "C" int athb_max_dti_bits(athb_ctx* c, unsigned long long* bits) {
+  if (!c || !bits) return athb_fail(ATHB_ERR_ARG, "null argument");
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  StepState h;
+  int rc = athb_read_clock(c, &h);
+  if (rc) return rc;
+  *bits = h.max_dti_bits;
+  return ATHB_OK;
+}
+
+// Impose the (global) maximum and apply the dt rule: after a step (after_step
+// != 0: time += dt, nstep++, then the new dt, and the state of the other
+// buffer becomes current) or before the loop (the first dt).
+extern "C" int athb_finish_step(athb_ctx* c, unsigned long long max_dti_bits, int after_step) {
+  if (!c) return athb_fail(ATHB_ERR_ARG, "null context");
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  k_set_max_dti<<<1, 1, 0, c->stream>>>(c->st, max_dti_bits);
+  k_finalize<<<1, 1, 0, c->stream>>>(c->st, c->dx1, c->dx2, after_step ? 1 : 0);
+  CUDA_TRY(cudaGetLastError());
+  if (after_step) c->cur ^= 1;
+  return ATHB_OK;
+}
+
+// Ghost fill of the resident state: mode 1 the x1 boundaries (on the
+// interior rows), 2 the x2 boundaries (whole rows), 3 both in that order;
+// sides bit 0 the inner, bit 1 the outer boundary of that direction.
+extern "C" int athb_ghost_fill(athb_ctx* c, int mode, int sides) {
+  if (!c || mode < 1 || mode > 3 || sides < 0 || sides > 3) return athb_fail(ATHB_ERR_ARG, "bad arguments");
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  if (mode == 3) {
+    int rc = athb_launch_ghost_phase(c, c->cur, 1, sides);
+    return rc ? rc : athb_launch_ghost_phase(c, c->cur, 2, sides);
+  }
+  return athb_launch_ghost_phase(c, c->cur, mode, sides);
+}
+
+// Rows [j0, j0+nrows) of all 11 planes of the resident state, ghost columns
+// included, to / from a host buffer laid out [plane][row][Nx1+8].
+static int rows_copy(athb_ctx* c, int j0, int nrows, double* host, bool to_host) {
+  if (!c || !host || j0 < 0 || nrows < 1 || j0 + nrows > c->sy) return athb_fail(ATHB_ERR_ARG, "bad row range");
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  double* dev = c->state[c->cur] + (size_t)j0 * c->pitch;
+  const size_t w = sizeof(double) * c->sx;
+  for (int p = 0; p < NSTATE; p++) {
+    double* h = host + (size_t)p * nrows * c->sx;
+    double* d = dev + (size_t)p * c->ps;
+    if (to_host)
+      CUDA_TRY(cudaMemcpy2DAsync(h, w, d, sizeof(double) * c->pitch, w, nrows, cudaMemcpyDeviceToHost, c->stream));
+    else
+      CUDA_TRY(cudaMemcpy2DAsync(d, sizeof(double) * c->pitch, h, w, w, nrows, cudaMemcpyHostToDevice, c->stream));
+  }
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return ATHB_OK;
+}
+extern "C" int athb_rows_get(athb_ctx* c, int j0, int nrows, double* host) {
+  return rows_copy(c, j0, nrows, host, true);
+}
+extern "C" int athb_rows_put(athb_ctx* c, int j0, int nrows, const double* host) {
+  return rows_copy(c, j0, nrows, const_cast<double*>(host), false);
+}

@@ -158,6 +158,23 @@ void *athb_stream(athb_ctx *ctx);
  * round trip per step.                                                      */
 int athb_set_pause(athb_ctx *ctx, double tpause, int on);
 
+/* ---- pieces of an iteration, for a grid split over several contexts ------ */
+/* A slab decomposition along x2 (one context per GPU, athena_cuda_b200/
+ * decomp.py) runs each iteration as: athb_integrate_local; a max across the
+ * contexts of athb_max_dti_bits; athb_finish_step(global max, 1); x1 ghosts
+ * (athb_ghost_fill mode 1); the exchange of 4 ghost rows with the
+ * neighbours (athb_rows_get / athb_rows_put); x2 ghosts at the global ends
+ * (mode 2).  No reference counterpart: the reference grid is one process
+ * (MPI_SERIAL).                                                             */
+int athb_set_geometry(athb_ctx *ctx, double dx1, double dx2, double x1_0, double x2_0);
+int athb_integrate_local(athb_ctx *ctx);
+int athb_cfl_local(athb_ctx *ctx);
+int athb_max_dti_bits(athb_ctx *ctx, unsigned long long *bits);
+int athb_finish_step(athb_ctx *ctx, unsigned long long max_dti_bits, int after_step);
+int athb_ghost_fill(athb_ctx *ctx, int mode, int sides);
+int athb_rows_get(athb_ctx *ctx, int j0, int nrows, double *host);
+int athb_rows_put(athb_ctx *ctx, int j0, int nrows, const double *host);
+
 /* Data dumps of the resident state, byte-identical to the reference's:
  * athb_dump_bin writes dump_binary's file (src/dump_binary.c:25-134; the
  * interior is converted to float on the GPU), athb_dump_tab dump_tab's
