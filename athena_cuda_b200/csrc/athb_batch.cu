@@ -725,7 +725,7 @@ static int launch_step(athb_batch* b) {
 }
 
 // Launch nsteps steps without synchronising (persistent: one cooperative
-// launch each, captured in a CUDA graph when the driver allows it; phased:
+// launch each, captured in a CUDA graph when CUDA accepts the capture; phased:
 // six launches each).
 extern "C" int athb_batch_run_async(athb_batch* b, int nsteps) {
   if (!b || nsteps < 0) return athb_fail(ATHB_ERR_ARG, "bad arguments");

@@ -1,5 +1,5 @@
 """Size-independent properties of the GPU step and the reference's own
-physics checks (SURVEY §8(c)): constrained transport keeps div B at
+physics checks: constrained transport keeps div B at
 round-off on every step; periodic runs conserve mass and energy to
 round-off; the circularly polarised Alfven wave converges at second order
 and its L1 errors equal the reference's Userwork_after_loop output
