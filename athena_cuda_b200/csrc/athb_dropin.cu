@@ -39,6 +39,7 @@ struct DropIn {
   int bc[4] = {0, 0, 0, 0};
   bool bc_set = false;
   int flux = ATHB_FLUX_ROE;
+  int device = -1;  // < 0: ATHB_DEVICE from the environment, else 0
   athb_VBCFun_t user_bc[4] = {nullptr, nullptr, nullptr, nullptr};
   std::vector<void*> registered;
   unsigned long long h2d = 0, d2h = 0;  // bytes moved by the drop-in calls
@@ -121,7 +122,11 @@ athb_ctx* context_for(athb_Grid* pG, const char* where) {
     cfg.gamma = Gamma > 1.0 ? Gamma : 5.0 / 3.0;
     cfg.cour_no = CourNo; cfg.tlim = 0.0; cfg.nlim = -1;
     cfg.flux = d.flux;
-    cfg.device = 0;
+    cfg.device = d.device;
+    if (cfg.device < 0) {
+      const char* env = getenv("ATHB_DEVICE");  // one process per GPU without a code change
+      cfg.device = env ? atoi(env) : 0;
+    }
     check(athb_create(&cfg, &d.ctx), where);
   }
   athb_ctx* c = d.ctx;
@@ -237,6 +242,16 @@ extern "C" void athb_dropin_set_bc(int ibc_x1, int obc_x1, int ibc_x2, int obc_x
 extern "C" void athb_dropin_bytes(unsigned long long* h2d, unsigned long long* d2h) {
   if (h2d) *h2d = g_drop.h2d;
   if (d2h) *d2h = g_drop.d2h;
+}
+
+// The GPU the drop-in calls use (set before the first call; default: the
+// ATHB_DEVICE environment variable, else device 0).
+extern "C" void athb_dropin_set_device(int device) {
+  if (g_drop.ctx && g_drop.ctx->cfg.device != device) {
+    athb_destroy(g_drop.ctx);
+    g_drop.ctx = nullptr;
+  }
+  g_drop.device = device;
 }
 
 extern "C" void athb_dropin_set_flux(int flux) {

@@ -322,11 +322,11 @@ def ours(a) -> None:
             "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (field-loop initial condition, src/field_loop.c)",
-            "config": config_dict(a), "gpu_launches": 7 * a.steps, "roofline": roofline,
+            "config": config_dict(a), "gpu_launches": 7 * a.steps * ws, "roofline": roofline,
             "clocks": clk.summary()}
 
-    if rank == 0 and not a.no_e2e:
-        line["e2e"] = e2e(a, ath)
+    if not a.no_e2e:
+        line["e2e"] = e2e(a, ath, local, ws)  # every rank: a collective for N > 1
     if rank == 0 and ws == 1 and not a.no_cpu and ref_exe().exists():
         r = run_ref_sample(ath, a.cpu_steps, 1, td)
         line["cpu_baseline"] = {"value": r["value"], "unit": UNIT, "cores": 1, "kind": "reference",
@@ -338,9 +338,11 @@ def ours(a) -> None:
         torch.distributed.destroy_process_group()
 
 
-def e2e(a, ath: Path) -> dict:
+def e2e(a, ath: Path, device: int = 0, ws: int = 1) -> dict:
     """The same metric through the reference-named drop-in ABI: the host Grid
-    (pinned) is the state; every step copies it to the GPU and the result back."""
+    (pinned) is the state; every step copies it to the GPU and the result back.
+    With ws ranks each runs its own replica on its GPU (collective: the
+    whole-job value uses the slowest rank's time)."""
     from athena_cuda_b200 import Params, configs, problem_state
     from athena_cuda_b200.dropin import DropInLoop, HostGrid
 
@@ -349,7 +351,7 @@ def e2e(a, ath: Path) -> dict:
     planes = problem_state("field_loop", p)
     dx1, dx2 = (cfg.x1max - cfg.x1min) / cfg.nx1, (cfg.x2max - cfg.x2min) / cfg.nx2
     hg = HostGrid(planes, dx1, dx2, cfg.x1min, cfg.x2min)
-    loop = DropInLoop(hg, configs.GAMMA, cfg.cour_no, bc=(4, 4, 4, 4))
+    loop = DropInLoop(hg, configs.GAMMA, cfg.cour_no, bc=(4, 4, 4, 4), device=device)
     loop.steps(2)  # warm-up
     h0, d0 = loop.bytes_moved()
     t0 = time.perf_counter()
@@ -358,7 +360,10 @@ def e2e(a, ath: Path) -> dict:
     h1, d1 = loop.bytes_moved()
     loop.close()
     hg.close()
-    return {"value": a.nx * a.ny * n / dt, "unit": UNIT, "h2d_bytes_per_step": (h1 - h0) // n,
+    if ws > 1:
+        import torch
+        dt = max_over_ranks(dt, ws, torch.device("cuda", device))
+    return {"value": ws * a.nx * a.ny * n / dt, "unit": UNIT, "h2d_bytes_per_step": (h1 - h0) // n,
             "d2h_bytes_per_step": (d1 - d0) // n, "steps": n,
             "path": "integrate_2d + new_dt + set_bvals drop-in calls on a pinned host Grid"}
 

@@ -308,6 +308,9 @@ int athb_integrate_noalloc(const athb_config *cfg, const double *d_in, double *d
 
 /* Drop-in configuration without the host program's par.c.                  */
 void athb_dropin_set_bc(int ibc_x1, int obc_x1, int ibc_x2, int obc_x2);
+/* GPU used by the drop-in calls (before the first call; default: the
+ * ATHB_DEVICE environment variable, else 0).                                */
+void athb_dropin_set_device(int device);
 void athb_dropin_set_flux(int flux);
 /* Bytes the drop-in entry points have copied host->device / device->host.  */
 void athb_dropin_bytes(unsigned long long *h2d, unsigned long long *d2h);
