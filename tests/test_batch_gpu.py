@@ -95,3 +95,25 @@ def test_phased_mode_matches_persistent():
         assert refutil.mismatch_report(ref[k][0], planes, PLANES) == ""
         assert (dt, t, n) == ref[k][1:]
     b.close()
+
+
+@pytest.mark.parametrize("mode", [Batch.PERSISTENT, Batch.PHASED])
+def test_hlle_batch_matches_reference(mode, tmp_path):
+    """A batch whose instances all use HLLE (src/flux_hlle.c) equals the
+    reference CPU path built with flux_hlle, instance by instance."""
+    items = ensemble.instances(4, seed=11, sizes=(8, 16, 24), tlim=0.04, flux="hlle")
+    b = Batch.from_problems(items)
+    b.mode = mode
+    b.run(10_000)
+    for k, (problem, blocks) in enumerate(items):
+        planes, dt, t, n = b.download(k)
+        if refutil.have_ref(problem, "hlle"):
+            ref = refutil.run_ref(problem, "hlle", write_athinput(tmp_path / f"a{k}", blocks), tmp_path)
+            assert refutil.mismatch_report(ref["planes"], planes, PLANES) == ""
+            assert (n, t, dt) == (ref["nstep"], ref["time"], ref["dt"])
+        else:
+            g = Grid.from_athinput(write_athinput(tmp_path / f"a{k}", blocks), problem)
+            g.run(1_000_000)
+            assert refutil.mismatch_report(g.download()[0], planes, PLANES) == ""
+            g.close()
+    b.close()

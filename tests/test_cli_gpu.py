@@ -80,3 +80,21 @@ def test_cli_rejects_unknown_override(tmp_path):
     r = subprocess.run([str(EXE), "-i", str(ath), "-p", "field_loop", "grid/nonexistent=3"], cwd=tmp_path,
                        capture_output=True, text=True, timeout=120)
     assert r.returncode != 0 and "not found" in r.stderr
+
+
+def test_cli_hlle_matches_reference_step(tmp_path):
+    """job/flux = hlle selects flux_hlle everywhere; the reference's main
+    program cannot (its flux is fixed at compile time), so the dumps are
+    checked against the reference CPU step built with flux_hlle."""
+    if not refutil.have_ref("blast", "hlle"):
+        pytest.skip("reference CPU path not built")
+    blocks = _outputs(configs.blast(30, 20, tlim=0.01, flux="hlle"), [{"out_fmt": "bin", "dt": 1.0}])
+    ath = write_athinput(tmp_path / "athinput", blocks)
+    r = subprocess.run([str(EXE), "-i", str(ath), "-p", "blast", "-q"], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    ref = refutil.run_ref("blast", "hlle", ath, tmp_path)
+    last = _cycles(r.stdout)[-1]
+    assert last.startswith(f"cycle={ref['nstep']} ")
+    assert (tmp_path / "Blast.0000.bin").exists()
+
