@@ -143,6 +143,23 @@ def run_ref_sample(ath: Path, steps: int, procs: int, workdir: Path, max_seconds
             "seconds": max(o["seconds"] for o in outs)}
 
 
+def run_ref_instances(aths: list[Path], problem: str, workdir: Path, max_seconds: float = 20.0) -> dict:
+    """One single-threaded reference process per athinput, all at once, each
+    running its instance to its end time (or for max_seconds of main loop);
+    zone-cycles/s summed over processes."""
+    exe = ROOT / "oracle" / "_ref" / f"athref_{problem}_roe"
+    ps = [subprocess.Popen([str(exe), "-i", str(ath), "--steps", "1000000000", "--bench", "--max-seconds",
+                            str(max_seconds)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, cwd=workdir,
+                           text=True) for ath in aths]
+    outs = []
+    for p in ps:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            raise RuntimeError("reference run failed")
+        outs.append(json.loads(out.strip().splitlines()[-1]))
+    return {"value": sum(o["zone_cycles_per_s"] for o in outs), "seconds": max(o["seconds"] for o in outs)}
+
+
 def cpu_model() -> str:
     try:
         for line in open("/proc/cpuinfo"):
@@ -472,6 +489,20 @@ def ensemble_arm(a) -> None:
             "speedup_vs_sequential": (seq_s * scale) / batched_s,
             "sequential_plain_s": plain_s * scale, "speedup_vs_sequential_plain": (plain_s * scale) / batched_s,
             "sequential_sample_stride": stride, "bit_exact_spot_checks": checked}
+    ref = ROOT / "oracle" / "_ref" / "athref_blast_roe"
+    if ref.exists():
+        # the reference CPU path, one process per host core (up to 16, each
+        # ~10 MB per instance), on the first instances of the same ensemble
+        from athena_cuda_b200 import write_athinput
+
+        cores = max(1, min(os.cpu_count() or 1, 16))
+        with tempfile.TemporaryDirectory() as td:
+            aths = [write_athinput(Path(td) / f"athinput.{k}", items[k][1]) for k in range(cores)]
+            r = run_ref_instances(aths, "blast", Path(td))
+        line["cpu_baseline"] = {"value": r["value"], "unit": UNIT, "cores": cores, "kind": "reference",
+                                "sample": f"instances 0..{cores - 1} of the ensemble, one single-threaded "
+                                          f"reference process each (-O2 -ffp-contract=off), up to 20 s of "
+                                          f"main loop each; {cpu_model()}"}
     print(json.dumps(line))
 
 
