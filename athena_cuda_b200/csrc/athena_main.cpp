@@ -37,7 +37,8 @@ void usage(const char* prog) {
   fprintf(stderr,
           "\nUsage: %s [options] [block/par=value ...]\n\nOptions:\n"
           "  -i <file>       Alternate input file [athinput]\n"
-          "  -p <problem>    Problem generator: blast, field_loop, cpaw2d [<job>/problem]\n"
+          "  -p <problem>    Problem generator: blast, field_loop, cpaw2d [<job>/problem, or\n"
+          "                  the --with-problem= of <comment>/config]\n"
           "  -d <directory>  Directory the outputs are written to [.]\n"
           "  -q              Print no cycle lines; run between outputs without host round trips\n"
           "  -h              This help\n",
@@ -134,12 +135,22 @@ int main(int argc, char** argv) {
   for (const char* o : overrides)
     if (athb_params_override(p, o)) die("par_cmdline");
   if (problem.empty()) {
-    const char* pj = athb_params_gets(p, "job", "problem");
-    if (!pj) {
-      fprintf(stderr, "[main]: no problem generator: give -p <problem> or <job>/problem\n");
+    // <job>/problem, else the configure line the reference's own athinput
+    // files carry in <comment> ("config = --with-problem=blast")
+    if (const char* pj = athb_params_gets(p, "job", "problem")) {
+      problem = pj;
+    } else if (const char* cf = athb_params_gets(p, "comment", "config")) {
+      const char* w = strstr(cf, "--with-problem=");
+      if (w) {
+        w += strlen("--with-problem=");
+        problem.assign(w, strcspn(w, " \t"));
+      }
+    }
+    if (problem.empty()) {
+      fprintf(stderr, "[main]: no problem generator: give -p <problem>, <job>/problem or "
+                      "<comment>/config = --with-problem=<name>\n");
       return 1;
     }
-    problem = pj;
   }
   const char* pid = athb_params_gets(p, "job", "problem_id");
   if (!pid) {

@@ -98,3 +98,19 @@ def test_cli_hlle_matches_reference_step(tmp_path):
     assert last.startswith(f"cycle={ref['nstep']} ")
     assert (tmp_path / "Blast.0000.bin").exists()
 
+
+
+def test_cli_takes_problem_from_comment_config(tmp_path):
+    """Without -p the problem comes from <comment> config = --with-problem=...,
+    the configure line of the reference's own athinput files."""
+    blocks = {"comment": {"problem": "Blast wave", "config": "--with-problem=blast"}}
+    blocks.update(_outputs(configs.blast(24, 16, tlim=0.01), [{"out_fmt": "tab", "dt": 0.005}]))
+    ath = write_athinput(tmp_path / "athinput", blocks)
+    outs = {}
+    for name, extra in {"p": ["-p", "blast"], "comment": []}.items():
+        d = tmp_path / name
+        d.mkdir()
+        r = subprocess.run([str(EXE), "-i", str(ath), *extra], cwd=d, capture_output=True, text=True, timeout=120)
+        assert r.returncode == 0, r.stderr
+        outs[name] = (_cycles(r.stdout), _files(d))
+    assert outs["p"] == outs["comment"] and outs["p"][1]
