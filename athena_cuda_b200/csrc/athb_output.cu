@@ -58,8 +58,9 @@ extern "C" int athb_dump_bin(athb_ctx* c, const char* path) {
   if (rc) return rc;
   const int nx1 = c->cfg.nx1, nx2 = c->cfg.nx2;
   const size_t n = (size_t)nx1 * nx2;
-  float* dbuf = nullptr;
-  CUDA_TRY(cudaMalloc(&dbuf, 8 * n * sizeof(float)));
+  // 8 floats per cell fit in the first 4 scratch planes, which hold nothing
+  // between steps (the dump runs on the context's stream, after the step)
+  float* dbuf = reinterpret_cast<float*>(c->scr);
   std::vector<float> data(8 * n);
   const long long blocks = std::min<long long>((8 * (long long)n + kThreads - 1) / kThreads, 148LL * 16);
   k_interior_float<<<(int)blocks, kThreads, 0, c->stream>>>(c->state[c->cur], c->ps, c->pitch, c->is, c->js, nx1,
@@ -68,7 +69,6 @@ extern "C" int athb_dump_bin(athb_ctx* c, const char* path) {
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(data.data(), dbuf, data.size() * sizeof(float), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  cudaFree(dbuf);
   if (e != cudaSuccess) return athb_fail(ATHB_ERR_CUDA, "athb_dump_bin: %s", cudaGetErrorString(e));
 
   FILE* f = fopen(path, "wb");

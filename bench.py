@@ -72,7 +72,7 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="field_loop", choices=["field_loop", "ensemble"])
+    ap.add_argument("--workload", default="field_loop", choices=["field_loop", "ensemble", "cpaw"])
     ap.add_argument("--ensemble-n", type=int, default=512)
     ap.add_argument("--seq-sample", type=int, default=0,
                     help="time sequential single-grid runs on every k-th instance only (0: all)")
@@ -506,6 +506,48 @@ def ensemble_arm(a) -> None:
     print(json.dumps(line))
 
 
+def cpaw_arm(a) -> None:
+    """The circularly polarised Alfven wave over one period (32x16 .. 512x256,
+    Roe and HLLE): L1 error against the initial state (src/cpaw2d.c:222-302)
+    on the GPU, its convergence order, the reference CPU path's own L1 output
+    beside it (oracle/_ref, when built), and the GPU time per run."""
+    import torch
+
+    from athena_cuda_b200 import Grid, configs, write_athinput
+
+    sizes = [(32, 16), (64, 32), (128, 64), (256, 128), (512, 256)]
+    rows = []
+    with tempfile.TemporaryDirectory() as td:
+        for flux in ("roe", "hlle"):
+            prev = None
+            for nx1, nx2 in sizes:
+                d = Path(td) / f"{flux}_{nx1}"
+                d.mkdir()
+                ath = write_athinput(d / "athinput", configs.cpaw2d(nx1, nx2, flux=flux))
+                g = Grid.from_athinput(ath, "cpaw2d")
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                g.run(1_000_000)
+                wall = time.perf_counter() - t0
+                err = [float(x) for x in g.cpaw2d_errors()]
+                n = g.status()["nstep"]
+                g.close()
+                row = {"flux": flux, "nx1": nx1, "nx2": nx2, "steps": n, "gpu_s": wall, "l1_rms": err[0],
+                       "order": None if prev is None else math.log2(prev / err[0])}
+                exe = ROOT / "oracle" / "_ref" / f"athref_cpaw2d_{flux}"
+                if exe.exists():
+                    subprocess.run([str(exe), "-i", str(ath), "--l1", "--quiet"], cwd=d, check=True,
+                                   capture_output=True)
+                    last = [l for l in (d / "cpaw2d-errors.dat").read_text().splitlines() if not l.startswith("#")][-1]
+                    ref_rms = float(last.split()[2])
+                    row["ref_l1_rms"] = ref_rms
+                    row["same_to_6_digits"] = float(f"{err[0]:e}") == ref_rms
+                rows.append(row)
+                prev = err[0]
+    print(json.dumps({"workload": "cpaw2d convergence, one period (t = 1/sqrt(5)), Roe and HLLE",
+                      "metric": "L1 RMS error vs the initial state", "rows": rows}))
+
+
 def measured_hbm_gbs():
     """HBM copy bandwidth measured on this GPU pool (MEASURED_PEAKS.json)."""
     f = ROOT / "MEASURED_PEAKS.json"
@@ -521,6 +563,8 @@ def main():
         reference_arm(a)
     elif a.workload == "ensemble":
         ensemble_arm(a)
+    elif a.workload == "cpaw":
+        cpaw_arm(a)
     else:
         ours(a)
 
