@@ -72,7 +72,7 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="field_loop", choices=["field_loop", "ensemble", "cpaw"])
+    ap.add_argument("--workload", default="field_loop", choices=["field_loop", "ensemble", "cpaw", "configs"])
     ap.add_argument("--ensemble-n", type=int, default=512)
     ap.add_argument("--seq-sample", type=int, default=0,
                     help="time sequential single-grid runs on every k-th instance only (0: all)")
@@ -122,12 +122,13 @@ def ref_exe() -> Path:
     return ROOT / "oracle" / "_ref" / "athref_field_loop_roe"
 
 
-def run_ref_sample(ath: Path, steps: int, procs: int, workdir: Path, max_seconds: float = 25.0) -> dict:
+def run_ref_sample(ath: Path, steps: int, procs: int, workdir: Path, max_seconds: float = 25.0,
+                   exe: Path | None = None) -> dict:
     """`procs` concurrent single-threaded reference processes, each running
     `steps` main-loop iterations (or fewer once its loop has run max_seconds);
     zone-cycles/s summed over processes (each process times its own main loop,
     setup excluded)."""
-    exe = ref_exe()
+    exe = exe or ref_exe()
     ps = [subprocess.Popen([str(exe), "-i", str(ath), "--steps", str(steps), "--bench",
                             "--max-seconds", str(max_seconds)],
                            stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, cwd=workdir, text=True)
@@ -548,6 +549,51 @@ def cpaw_arm(a) -> None:
                       "metric": "L1 RMS error vs the initial state", "rows": rows}))
 
 
+def configs_arm(a) -> None:
+    """Every plain configuration of the reference's benchmark set run to its
+    end time on the GPU (device-resident loop, CUDA events), beside the
+    reference CPU path on one core (the whole run when it takes under ~30 s,
+    else a bounded number of steps)."""
+    import torch
+
+    from athena_cuda_b200 import Grid, configs, write_athinput
+
+    cases = [
+        ("blast 200x300 to t=0.2", "blast", configs.blast(200, 300), None),
+        ("field loop 1024x512 to t=1", "field_loop", configs.field_loop(1024, 512), 20),
+        ("field loop 2048x2048 to t=1", "field_loop", configs.field_loop(2048, 2048), 3),
+    ]
+    rows = []
+    with tempfile.TemporaryDirectory() as td:
+        for label, problem, blocks, ref_steps in cases:
+            d = Path(td) / problem
+            d.mkdir(exist_ok=True)
+            ath = write_athinput(d / f"athinput.{len(rows)}", blocks)
+            g = Grid.from_athinput(ath, problem)
+            stream = torch.cuda.ExternalStream(g.stream)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            g.run(10_000_000)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            st = g.status()
+            g.close()
+            cells = blocks["grid"]["Nx1"] * blocks["grid"]["Nx2"]
+            gpu = cells * st["nstep"] / (e0.elapsed_time(e1) * 1e-3)
+            row = {"config": label, "steps": st["nstep"], "time": st["time"], "gpu_s": e0.elapsed_time(e1) * 1e-3,
+                   "gpu_zc_per_s": gpu}
+            exe = ROOT / "oracle" / "_ref" / f"athref_{problem}_roe"
+            if exe.exists():
+                r = run_ref_sample(ath, ref_steps or 10_000_000, 1, d, max_seconds=30.0, exe=exe)
+                row.update(ref_zc_per_s=r["value"], ref_seconds=r["seconds"],
+                           ref_sample="whole run" if ref_steps is None else f"{ref_steps} steps",
+                           speedup=gpu / r["value"])
+            rows.append(row)
+    print(json.dumps({"workload": "plain configurations to their end times, Roe, FP64", "unit": UNIT,
+                      "cpu": cpu_model(), "rows": rows}))
+
+
 def measured_hbm_gbs():
     """HBM copy bandwidth measured on this GPU pool (MEASURED_PEAKS.json)."""
     f = ROOT / "MEASURED_PEAKS.json"
@@ -565,6 +611,8 @@ def main():
         ensemble_arm(a)
     elif a.workload == "cpaw":
         cpaw_arm(a)
+    elif a.workload == "configs":
+        configs_arm(a)
     else:
         ours(a)
 
