@@ -15,7 +15,7 @@ from __future__ import annotations
 import json
 from pathlib import Path
 
-LY_CANDIDATES = (4, 8, 16, 32, 64)
+LY_CANDIDATES = (2, 4, 8, 16, 32, 64)
 TARGET_CELLS = 4_000_000
 
 

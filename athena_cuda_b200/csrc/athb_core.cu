@@ -112,9 +112,12 @@ extern "C" int athb_create(const athb_config* cfg, athb_ctx** out) {
   c->dx2 = (cfg->x2max - cfg->x2min) / (double)cfg->nx2;
   c->x1_0 = cfg->x1min; c->x2_0 = cfg->x2min;
   {
-    long long cols = cfg->nx1 + 4, faces = cfg->nx2 + 3;
-    long long ly = (cols * faces) / (148LL * 512);
-    c->ly = (int)std::max(4LL, std::min(64LL, ly));
+    // rows per column march: short marches on small grids, where the step
+    // is latency-bound and more threads shorten it (64^2 and 128^2 run
+    // fastest at 1, 200x300 at 2-3), else enough marches for ~512 threads
+    // per SM (measured on B200, blast and field loop)
+    const long long cf = (long long)(cfg->nx1 + 4) * (cfg->nx2 + 3);
+    c->ly = cf < 40000 ? 1 : cf < 100000 ? 2 : (int)std::max(4LL, std::min(64LL, cf / (148LL * 512)));
   }
   cudaError_t e = cudaSetDevice(cfg->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);

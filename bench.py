@@ -452,7 +452,7 @@ def ensemble_arm(a) -> None:
         g.set_bvals()
         g.new_dt()
         if sizes[k] not in iso_ly:
-            best, _ = min(((ly, _time_ly(g, ly)) for ly in (2, 4, 8, 16, 32) if ly <= sizes[k][1] + 3),
+            best, _ = min(((ly, _time_ly(g, ly)) for ly in (1, 2, 4, 8, 16, 32) if ly <= sizes[k][1] + 3),
                           key=lambda x: x[1])
             iso_ly[sizes[k]] = best
             g.upload(problem_state(name, p))  # the trials advanced the grid
