@@ -32,3 +32,28 @@ def instances(n: int = 512, seed: int = 2024, sizes=SIZES, tlim: float = 0.1,
         out.append(("blast", configs.blast(nx1, nx2, tlim=tlim, prat=prat, radius=radius, b0=b0,
                                            angle=angle, flux=flux)))
     return out
+
+
+def work_estimate(blocks: dict) -> float:
+    """Relative cost of one instance run to its end time: cells times steps,
+    the steps taken as proportional to the cells across the smaller cell
+    width (the CFL step shrinks with the cell size)."""
+    g = blocks["grid"]
+    dx = min((g["x1max"] - g["x1min"]) / g["Nx1"], (g["x2max"] - g["x2min"]) / g["Nx2"])
+    return g["Nx1"] * g["Nx2"] * blocks["time"]["tlim"] / dx
+
+
+def partition(items: list[tuple[str, dict]], ranks: int) -> list[list[int]]:
+    """Instance indices per rank (one GPU each), balanced by work_estimate:
+    largest first, each to the least-loaded rank.  The instances are
+    independent, so a partitioned ensemble needs no communication."""
+    if ranks < 1:
+        raise ValueError("ranks must be >= 1")
+    order = sorted(range(len(items)), key=lambda k: (-work_estimate(items[k][1]), k))
+    load = [0.0] * ranks
+    parts: list[list[int]] = [[] for _ in range(ranks)]
+    for k in order:
+        r = min(range(ranks), key=lambda q: (load[q], q))
+        parts[r].append(k)
+        load[r] += work_estimate(items[k][1])
+    return [sorted(p) for p in parts]

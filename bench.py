@@ -403,6 +403,10 @@ def ensemble_arm(a) -> None:
     from athena_cuda_b200 import Batch, Grid, Params, autotune, ensemble, problem_state
 
     items = ensemble.instances(a.ensemble_n, seed=2024)
+    ws, rank, local = dist_env()
+    if ws > 1:
+        ensemble_ranks(a, items, ws, rank, local)
+        return
     sizes = [(b["grid"]["Nx1"], b["grid"]["Nx2"]) for _, b in items]
     runs = {}
     for mode_name, mode in (("persistent", Batch.PERSISTENT), ("phased", Batch.PHASED)):
@@ -505,6 +509,58 @@ def ensemble_arm(a) -> None:
                                           f"reference process each (-O2 -ffp-contract=off), up to 20 s of "
                                           f"main loop each; {cpu_model()}"}
     print(json.dumps(line))
+
+
+def run_batch(items, local: int, mode: int):
+    """One Batch of `items` on GPU `local`, tuned, run to every end time;
+    (wall seconds, zone-cycles, final states)."""
+    import torch
+
+    from athena_cuda_b200 import Batch, autotune
+
+    for _, b in items:
+        b["job"]["device"] = local
+    sizes = [(b["grid"]["Nx1"], b["grid"]["Nx2"]) for _, b in items]
+    batch = Batch.from_problems(items)
+    batch.mode = mode
+    autotune.tune_batch(batch, sizes, cache=Path(tempfile.gettempdir()) / f"athb_ly_tuning_{local}.json")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    batch.run(100000)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    finals = [batch.download(k) for k in range(batch.n)]
+    batch.close()
+    return wall, sum(nx1 * nx2 * f[3] for (nx1, nx2), f in zip(sizes, finals)), finals
+
+
+def ensemble_ranks(a, items, ws: int, rank: int, local: int) -> None:
+    """The ensemble bin-packed over ws GPUs (ensemble.partition by estimated
+    work), each rank one phased Batch of its share, no communication but the
+    timing: whole-job zone-cycles/s over the slowest rank's time."""
+    import datetime
+
+    import torch
+
+    from athena_cuda_b200 import Batch, ensemble
+
+    torch.cuda.set_device(local)
+    torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                         device_id=torch.device("cuda", local))
+    mine = [items[k] for k in ensemble.partition(items, ws)[rank]]
+    torch.distributed.barrier()
+    wall, zc, _ = run_batch(mine, local, Batch.PHASED)
+    worst = max_over_ranks(wall, ws, torch.device("cuda", local))
+    t = torch.tensor([float(zc)], dtype=torch.float64, device=torch.device("cuda", local))
+    torch.distributed.all_reduce(t)
+    if rank == 0:
+        print(json.dumps({"metric": "ensemble zone-cycles/s (512 blast instances to t=0.1, batched)",
+                          "value": float(t.item()) / worst, "unit": UNIT, "n_gpus": ws, "scaling": "strong",
+                          "dtype": "f64", "data": "synthetic (seeded blast ensemble)",
+                          "config": {"workload": f"blast ensemble n={len(items)} sizes 64..512 per side",
+                                     "seed": 2024, "batch_mode": "phased", "parallelism": f"partitioned x{ws}"},
+                          "zone_cycles": float(t.item()), "batched_s": worst}))
+    torch.distributed.destroy_process_group()
 
 
 def cpaw_arm(a) -> None:
