@@ -104,27 +104,37 @@ __host__ __device__ inline int item_count(const InstGeom& I, int seg) {
   }
 }
 
-__device__ void grid_barrier(const BatchDev& B) {
+// Wait until `blocks` blocks have arrived.  A block that waits longer than
+// `spins` polls gives up: it sets *err and carries on, so a launch whose
+// blocks cannot all arrive ends with an error status instead of a hang.
+__device__ void grid_barrier_n(BarrierState* bar, int* err, unsigned int blocks, long long spins) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned int* vgen = &B.bar->gen;
+    volatile unsigned int* vgen = &bar->gen;
     const unsigned int gen = *vgen;
     __threadfence();
-    const unsigned int arrived = atomicAdd(&B.bar->count, 1u) + 1u;
-    if (arrived == gridDim.x) {
-      B.bar->count = 0u;
+    const unsigned int arrived = atomicAdd(&bar->count, 1u) + 1u;
+    if (arrived == blocks) {
+      bar->count = 0u;
       __threadfence();
-      atomicAdd(&B.bar->gen, 1u);
+      atomicAdd(&bar->gen, 1u);
     } else {
-      long long spins = 0;
+      long long n = 0;
       while (*vgen == gen) {
         __nanosleep(64);
-        if (++spins > kBarrierSpins) { atomicExch(B.err, 1); break; }
+        if (++n > spins) { atomicExch(err, 1); break; }
       }
     }
     __threadfence();
   }
   __syncthreads();
+}
+
+__device__ void grid_barrier(const BatchDev& B) { grid_barrier_n(B.bar, B.err, gridDim.x, kBarrierSpins); }
+
+// Self-test of the bounded wait: one block waits for two at a barrier.
+__global__ void k_barrier_selftest(BarrierState* bar, int* err, long long spins) {
+  grid_barrier_n(bar, err, 2u, spins);
 }
 
 // Copy instance k's geometry into shared memory (all threads), with the
@@ -829,6 +839,33 @@ extern "C" int athb_batch_timing(athb_batch* b, int enable, double* ms_out) {
 }
 
 extern "C" int athb_batch_grid(const athb_batch* b) { return b ? b->grid : 0; }
+
+// The failure path of the batch's grid barrier, on purpose: a single block
+// waits at a barrier for two, gives up after `spins` polls (~64 ns each),
+// records the time-out and returns; the device stays usable.  *timed_out is
+// 1 when the wait ran out (the expected outcome).
+extern "C" int athb_batch_selftest_barrier(int device, long long spins, int* timed_out) {
+  if (!timed_out || spins < 1) return athb_fail(ATHB_ERR_ARG, "bad arguments");
+  CUDA_TRY(cudaSetDevice(device));
+  BarrierState* bar = nullptr;
+  int* err = nullptr;
+  CUDA_TRY(cudaMalloc(&bar, sizeof(BarrierState)));
+  cudaError_t e = cudaMalloc(&err, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(bar, 0, sizeof(BarrierState));
+  if (e == cudaSuccess) e = cudaMemset(err, 0, sizeof(int));
+  if (e == cudaSuccess) {
+    k_barrier_selftest<<<1, kThreads>>>(bar, err, spins);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  int h = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(bar);
+  cudaFree(err);
+  if (e != cudaSuccess) return athb_fail(ATHB_ERR_CUDA, "barrier self-test: %s", cudaGetErrorString(e));
+  *timed_out = h;
+  return ATHB_OK;
+}
 
 // Execution mode: ATHB_BATCH_PERSISTENT (one cooperative launch per step) or
 // ATHB_BATCH_PHASED (one launch per phase).  Results are identical.

@@ -286,6 +286,10 @@ int athb_batch_timing(athb_batch *b, int enable, double *ms_out);
 #define ATHB_BATCH_PHASED 1
 int athb_batch_set_mode(athb_batch *b, int mode);
 int athb_batch_mode(const athb_batch *b);
+/* Failure-path self-test of the persistent kernel's grid barrier: one block
+ * waits for two, gives up after `spins` polls (~64 ns each), and the time-out
+ * is reported in *timed_out (1 expected) with the device still usable.      */
+int athb_batch_selftest_barrier(int device, long long spins, int *timed_out);
 
 /* ---- allocation-free step ------------------------------------------------ */
 /* No counterpart in the reference.  One integrate_2d step (the cells

@@ -70,3 +70,35 @@ def test_noalloc_rejects_grids_beyond_its_scratch(tmp_path):
     out = torch.zeros_like(buf)
     rc = _noalloc()(C.byref(cfg), buf.data_ptr(), out.data_ptr(), 1e-3, None)
     assert rc == 1 and b"5184" in lib().athb_last_error()
+
+
+def test_noalloc_writes_only_the_step_cells(tmp_path):
+    """Guard bands around the caller's output buffer, and every cell the step
+    does not write, keep a sentinel (a memory-safety check in place of a
+    sanitizer): only interior cells, B1i column ie+1 and B2i row je+1 change."""
+    import torch
+
+    blocks = configs.blast(30, 20, bc=(2, 2, 1, 1))
+    ath = write_athinput(tmp_path / "athinput", blocks)
+    g = Grid.from_athinput(ath, "blast")
+    planes, dt, _, _ = g.download()
+    g.close()
+    cfg = Params(ath).config()
+    guard, mark = 4096, 0x7FF4DEADBEEF0001
+    d_in = torch.tensor(planes, device="cuda")
+    out = torch.empty(2 * guard + planes.size, dtype=torch.float64, device="cuda")
+    out.view(torch.int64).fill_(mark)
+    rc = _noalloc()(C.byref(cfg), d_in.data_ptr(), out[guard:].data_ptr(), dt, None)
+    assert rc == 0, lib().athb_last_error().decode()
+    torch.cuda.synchronize()
+    bits = out.view(torch.int64).cpu().numpy()
+    assert (bits[:guard] == mark).all() and (bits[-guard:] == mark).all()
+    body = bits[guard:-guard].reshape(planes.shape)
+    written = np.zeros(planes.shape, dtype=bool)
+    is_, ie, js, je = 4, 4 + cfg.nx1 - 1, 4, 4 + cfg.nx2 - 1
+    written[:, js:je + 1, is_:ie + 1] = True
+    written[8, js:je + 1, ie + 1] = True   # B1i column ie+1
+    written[9, je + 1, is_:ie + 1] = True  # B2i row je+1
+    assert (body[~written] == mark).all(), "the step wrote outside its cells"
+    assert (body[written] != mark).all()
+
