@@ -35,7 +35,7 @@ CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", f"-I{ROOT / 'inc
 CU_SOURCES = ["athb_core.cu", "athb_dropin.cu", "athb_batch.cu", "athb_noalloc.cu", "athb_output.cu",
               "athb_problems_dev.cu"]
 CPP_SOURCES = ["athinput.cpp", "problems.cpp"]
-HEADERS = ["mhd_physics.cuh", "step_types.cuh", "step_kernels.cuh", "athb_internal.h"]
+HEADERS = ["dual.cuh", "mhd_physics.cuh", "step_types.cuh", "step_kernels.cuh", "athb_internal.h"]
 
 
 def _run(cmd: list[str], verbose: bool) -> str:

@@ -19,7 +19,10 @@
 //    at the start of every call;
 //  * the device address of the array is looked up (cudaGetSymbolAddress) on
 //    the first call made on each device, with that device current; make that
-//    first call before any stream capture.
+//    first call before any stream capture;
+//  * the step runs on the current device, which must be cfg->device;
+//  * no non-finite check: a NaN or negative-pressure step is not reported
+//    (the regular paths report it through athb_status / athb_run).
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -95,6 +98,14 @@ extern "C" int athb_integrate_noalloc(const athb_config* cfg, const double* d_in
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return athb_fail(ATHB_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+  // The step runs on the calling thread's current device (no cudaSetDevice
+  // here: switching devices is the caller's business mid-capture); a config
+  // naming another device is a caller error, not a silent redirect.
+  if (cfg->device != dev)
+    return athb_fail(ATHB_ERR_ARG,
+                     "athb_integrate_noalloc: cfg->device is %d but the current device is %d (make the "
+                     "device current with cudaSetDevice before the call)",
+                     cfg->device, dev);
   double* scratch = nullptr;
   rc = scratch_address(dev, &scratch);
   if (rc) return rc;

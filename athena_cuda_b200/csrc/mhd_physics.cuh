@@ -30,6 +30,8 @@
 
 #include <math.h>
 
+#include "dual.cuh"
+
 #if defined(__CUDACC__)
 #define ATHB_HD __host__ __device__ __forceinline__
 #else
@@ -43,41 +45,46 @@ constexpr double kTiny = 1.0e-20;   // TINY_NUMBER, src/defs.h:100
 // Conserved / primitive variables of one 1D slice, in the slice frame
 // (x = sweep direction).  Field order is that of Cons1D / Prim1D
 // (src/athena.h:75-98).
-struct Cons1 { double d, mx, my, mz, e, by, bz; };
-struct Prim1 { double d, vx, vy, vz, p, by, bz; };
+template <class T> struct Cons1T { T d, mx, my, mz, e, by, bz; };
+template <class T> struct Prim1T { T d, vx, vy, vz, p, by, bz; };
+using Cons1 = Cons1T<double>;
+using Prim1 = Prim1T<double>;
 
 // Equation-of-state constants (the reference globals Gamma, Gamma_1, Gamma_2).
 struct Eos { double gamma, gamma_1, gamma_2; };
 
 // MAX / MIN / SIGN exactly as the reference macros (src/defs.h:87-94).
-ATHB_HD double rmax(double a, double b) { return (a > b) ? a : b; }
-ATHB_HD double rmin(double a, double b) { return (a < b) ? a : b; }
-ATHB_HD double rsign(double a) { return (a < 0.) ? -1. : 1.; }
+template <class T> ATHB_HD T rmax(T a, T b) { return (a > b) ? a : b; }
+template <class T> ATHB_HD T rmin(T a, T b) { return (a < b) ? a : b; }
+template <class T> ATHB_HD T rsign(T a) { return (a < 0.) ? T(-1.) : T(1.); }
 
-ATHB_HD double cget(const Cons1& u, int n) {
+template <class T>
+ATHB_HD T cget(const Cons1T<T>& u, int n) {
   return n == 0 ? u.d : n == 1 ? u.mx : n == 2 ? u.my : n == 3 ? u.mz : n == 4 ? u.e : n == 5 ? u.by : u.bz;
 }
 
 // --- src/convert_var.c:37-55 -------------------------------------------------
-ATHB_HD Prim1 cons_to_prim(const Cons1& u, double bx, const Eos& eos) {
-  Prim1 w;
-  const double di = 1.0 / u.d;
+template <class T>
+ATHB_HD Prim1T<T> cons_to_prim(const Cons1T<T>& u, T bx, const Eos& eos) {
+  Prim1T<T> w;
+  const T di = 1.0 / u.d;
   w.d = u.d;
   w.vx = u.mx * di;
   w.vy = u.my * di;
   w.vz = u.mz * di;
-  double p = u.e - 0.5 * (u.mx * u.mx + u.my * u.my + u.mz * u.mz) * di;
+  T p = u.e - 0.5 * (u.mx * u.mx + u.my * u.my + u.mz * u.mz) * di;
   p -= 0.5 * (bx * bx + u.by * u.by + u.bz * u.bz);
   p *= eos.gamma_1;
-  w.p = rmax(p, kTiny);
+  w.p = rmax(p, T(kTiny));
   w.by = u.by;
   w.bz = u.bz;
   return w;
 }
 
 // --- src/convert_var.c:64-92 -------------------------------------------------
-ATHB_HD Cons1 prim_to_cons(const Prim1& w, double bx, const Eos& eos) {
-  Cons1 u;
+template <class T>
+ATHB_HD Cons1T<T> prim_to_cons(const Prim1T<T>& w, T bx, const Eos& eos) {
+  Cons1T<T> u;
   u.d = w.d;
   u.mx = w.d * w.vx;
   u.my = w.d * w.vy;
@@ -105,47 +112,49 @@ ATHB_HD Cons1 prim_to_cons(const Prim1& w, double bx, const Eos& eos) {
 //     row3: L30=1 L34=-1/asq ; row4 = (-L21,-L22,-L23, L24,L25,L26) ;
 //     row5 = (-L12,-L13, L15,L16) ; row6 = (-L01,-L02,-L03, L04,L05,L06)
 // ---------------------------------------------------------------------------
-struct PrimEig {
-  double ev[7];
-  double R00, R02, R10, R12, R20, R21, R22, R30, R31, R32, R40, R42, R50, R51, R52, R60, R61, R62;
-  double L01, L02, L03, L04, L05, L06, L12, L13, L15, L16, L21, L22, L23, L24, L25, L26, L34;
+template <class T> struct PrimEigT {
+  T ev[7];
+  T R00, R02, R10, R12, R20, R21, R22, R30, R31, R32, R40, R42, R50, R51, R52, R60, R61, R62;
+  T L01, L02, L03, L04, L05, L06, L12, L13, L15, L16, L21, L22, L23, L24, L25, L26, L34;
 };
+using PrimEig = PrimEigT<double>;
 
-ATHB_HD void esys_prim(double d, double v1, double p, double b1, double b2, double b3,
-                       const Eos& eos, PrimEig& E) {
-  const double di = 1.0 / d;
-  const double btsq = b2 * b2 + b3 * b3;
-  const double vaxsq = b1 * b1 * di;
-  const double asq = eos.gamma * p * di;
+template <class T>
+ATHB_HD void esys_prim(T d, T v1, T p, T b1, T b2, T b3,
+                       const Eos& eos, PrimEigT<T>& E) {
+  const T di = 1.0 / d;
+  const T btsq = b2 * b2 + b3 * b3;
+  const T vaxsq = b1 * b1 * di;
+  const T asq = eos.gamma * p * di;
 
-  const double ct2 = btsq * di;
-  const double tsum = vaxsq + ct2 + asq;
-  const double tdif = vaxsq + ct2 - asq;
-  const double cf2_cs2 = sqrt(tdif * tdif + 4.0 * asq * ct2);
-  const double cfsq = 0.5 * (tsum + cf2_cs2);
-  const double cf = sqrt(cfsq);
-  const double cssq = asq * vaxsq / cfsq;
-  const double cs = sqrt(cssq);
+  const T ct2 = btsq * di;
+  const T tsum = vaxsq + ct2 + asq;
+  const T tdif = vaxsq + ct2 - asq;
+  const T cf2_cs2 = sqrt(tdif * tdif + 4.0 * asq * ct2);
+  const T cfsq = 0.5 * (tsum + cf2_cs2);
+  const T cf = sqrt(cfsq);
+  const T cssq = asq * vaxsq / cfsq;
+  const T cs = sqrt(cssq);
 
-  const double bt = sqrt(btsq);
-  double bet2, bet3;
+  const T bt = sqrt(btsq);
+  T bet2, bet3;
   if (bt == 0.0) { bet2 = 1.0; bet3 = 0.0; } else { bet2 = b2 / bt; bet3 = b3 / bt; }
 
-  double alpha_f, alpha_s;
+  T alpha_f, alpha_s;
   if (cf2_cs2 == 0.0) { alpha_f = 1.0; alpha_s = 0.0; }
   else if ((asq - cssq) <= 0.0) { alpha_f = 0.0; alpha_s = 1.0; }
   else if ((cfsq - asq) <= 0.0) { alpha_f = 1.0; alpha_s = 0.0; }
   else { alpha_f = sqrt((asq - cssq) / cf2_cs2); alpha_s = sqrt((cfsq - asq) / cf2_cs2); }
 
-  const double sqrtd = sqrt(d);
-  const double s = rsign(b1);
-  const double a = sqrt(asq);
-  double qf = cf * alpha_f * s;
-  double qs = cs * alpha_s * s;
-  const double af = a * alpha_f * sqrtd;
-  const double as = a * alpha_s * sqrtd;
+  const T sqrtd = sqrt(d);
+  const T s = rsign(b1);
+  const T a = sqrt(asq);
+  T qf = cf * alpha_f * s;
+  T qs = cs * alpha_s * s;
+  const T af = a * alpha_f * sqrtd;
+  const T as = a * alpha_s * sqrtd;
 
-  const double vax = sqrt(vaxsq);
+  const T vax = sqrt(vaxsq);
   E.ev[0] = v1 - cf; E.ev[1] = v1 - vax; E.ev[2] = v1 - cs; E.ev[3] = v1;
   E.ev[4] = v1 + cs; E.ev[5] = v1 + vax; E.ev[6] = v1 + cf;
 
@@ -157,11 +166,11 @@ ATHB_HD void esys_prim(double d, double v1, double p, double b1, double b2, doub
   E.R50 = as * bet2;          E.R51 = -bet3 * s * sqrtd;  E.R52 = -af * bet2;
   E.R60 = as * bet3;          E.R61 = bet2 * s * sqrtd;   E.R62 = -af * bet3;
 
-  const double na = 0.5 / asq;
+  const T na = 0.5 / asq;
   qf = na * qf;
   qs = na * qs;
-  const double af_prime = na * af * di;
-  const double as_prime = na * as * di;
+  const T af_prime = na * af * di;
+  const T as_prime = na * as * di;
 
   E.L01 = -na * cf * alpha_f; E.L02 = qs * bet2; E.L03 = qs * bet3;
   E.L04 = na * alpha_f * di;  E.L05 = as_prime * bet2; E.L06 = as_prime * bet3;
@@ -174,16 +183,17 @@ ATHB_HD void esys_prim(double d, double v1, double p, double b1, double b2, doub
 
 // a = L * v for the primitive eigensystem, terms in the reference's column
 // order (src/lr_states_plm.c:122-133), exact zeros skipped.
-ATHB_HD void prim_project(const PrimEig& E, const double v[7], double a[7]) {
-  const double p01 = E.L01 * v[1], p02 = E.L02 * v[2], p03 = E.L03 * v[3];
-  const double p04 = E.L04 * v[4], p05 = E.L05 * v[5], p06 = E.L06 * v[6];
+template <class T>
+ATHB_HD void prim_project(const PrimEigT<T>& E, const T v[7], T a[7]) {
+  const T p01 = E.L01 * v[1], p02 = E.L02 * v[2], p03 = E.L03 * v[3];
+  const T p04 = E.L04 * v[4], p05 = E.L05 * v[5], p06 = E.L06 * v[6];
   a[0] = p01 + p02 + p03 + p04 + p05 + p06;
   a[6] = -p01 - p02 - p03 + p04 + p05 + p06;
-  const double p12 = E.L12 * v[2], p13 = E.L13 * v[3], p15 = E.L15 * v[5], p16 = E.L16 * v[6];
+  const T p12 = E.L12 * v[2], p13 = E.L13 * v[3], p15 = E.L15 * v[5], p16 = E.L16 * v[6];
   a[1] = p12 + p13 + p15 + p16;
   a[5] = -p12 - p13 + p15 + p16;
-  const double p21 = E.L21 * v[1], p22 = E.L22 * v[2], p23 = E.L23 * v[3];
-  const double p24 = E.L24 * v[4], p25 = E.L25 * v[5], p26 = E.L26 * v[6];
+  const T p21 = E.L21 * v[1], p22 = E.L22 * v[2], p23 = E.L23 * v[3];
+  const T p24 = E.L24 * v[4], p25 = E.L25 * v[5], p26 = E.L26 * v[6];
   a[2] = p21 + p22 + p23 + p24 + p25 + p26;
   a[4] = -p21 - p22 - p23 + p24 + p25 + p26;
   a[3] = v[0] + E.L34 * v[4];
@@ -191,7 +201,8 @@ ATHB_HD void prim_project(const PrimEig& E, const double v[7], double a[7]) {
 
 // One left eigenvector of the primitive system, as 7 coefficients (for the
 // characteristic tracing loop, src/lr_states_plm.c:201-224).
-ATHB_HD void prim_left_row(const PrimEig& E, int n, double l[7]) {
+template <class T>
+ATHB_HD void prim_left_row(const PrimEigT<T>& E, int n, T l[7]) {
   for (int m = 0; m < 7; m++) l[m] = 0.0;
   switch (n) {
   case 0: l[1] = E.L01; l[2] = E.L02; l[3] = E.L03; l[4] = E.L04; l[5] = E.L05; l[6] = E.L06; break;
@@ -205,7 +216,8 @@ ATHB_HD void prim_left_row(const PrimEig& E, int n, double l[7]) {
 }
 
 // One right eigenvector (column n) of the primitive system.
-ATHB_HD void prim_right_col(const PrimEig& E, int n, double r[7]) {
+template <class T>
+ATHB_HD void prim_right_col(const PrimEigT<T>& E, int n, T r[7]) {
   switch (n) {
   case 0: r[0] = E.R00; r[1] = E.R10;  r[2] = E.R20;  r[3] = E.R30;  r[4] = E.R40; r[5] = E.R50; r[6] = E.R60; break;
   case 1: r[0] = 0.0;   r[1] = 0.0;    r[2] = E.R21;  r[3] = E.R31;  r[4] = 0.0;   r[5] = E.R51; r[6] = E.R61; break;
@@ -233,17 +245,18 @@ ATHB_HD int prim_right_mask(int n) {  // column n
 // Returns wl_next = W_L at face i+1/2 (reference Wl[i+1]) and
 //         wr_this = W_R at face i-1/2 (reference Wr[i]).
 // ---------------------------------------------------------------------------
-ATHB_HD void plm_cell(const Prim1& wm, const Prim1& w0, const Prim1& wp, double bxc,
-                      double dtodx, const Eos& eos, Prim1& wl_next, Prim1& wr_this) {
-  PrimEig E;
+template <class T>
+ATHB_HD void plm_cell(const Prim1T<T>& wm, const Prim1T<T>& w0, const Prim1T<T>& wp, T bxc,
+                      T dtodx, const Eos& eos, Prim1T<T>& wl_next, Prim1T<T>& wr_this) {
+  PrimEigT<T> E;
   esys_prim(w0.d, w0.vx, w0.p, bxc, w0.by, w0.bz, eos, E);
 
-  const double Wm[7] = {wm.d, wm.vx, wm.vy, wm.vz, wm.p, wm.by, wm.bz};
-  const double W0[7] = {w0.d, w0.vx, w0.vy, w0.vz, w0.p, w0.by, w0.bz};
-  const double Wp[7] = {wp.d, wp.vx, wp.vy, wp.vz, wp.p, wp.by, wp.bz};
+  const T Wm[7] = {wm.d, wm.vx, wm.vy, wm.vz, wm.p, wm.by, wm.bz};
+  const T W0[7] = {w0.d, w0.vx, w0.vy, w0.vz, w0.p, w0.by, w0.bz};
+  const T Wp[7] = {wp.d, wp.vx, wp.vy, wp.vz, wp.p, wp.by, wp.bz};
 
   // Step 2: centred, left, right and van Leer differences.
-  double dWc[7], dWl[7], dWr[7], dWg[7];
+  T dWc[7], dWl[7], dWr[7], dWg[7];
 #pragma unroll
   for (int n = 0; n < 7; n++) {
     dWc[n] = Wp[n] - Wm[n];
@@ -254,26 +267,26 @@ ATHB_HD void plm_cell(const Prim1& wm, const Prim1& w0, const Prim1& wp, double 
   }
 
   // Step 3: characteristic projections.
-  double dac[7], dal[7], dar[7], dag[7];
+  T dac[7], dal[7], dar[7], dag[7];
   prim_project(E, dWc, dac);
   prim_project(E, dWl, dal);
   prim_project(E, dWr, dar);
   prim_project(E, dWg, dag);
 
   // Step 4: monotonicity constraints.
-  double da[7];
+  T da[7];
 #pragma unroll
   for (int n = 0; n < 7; n++) {
     da[n] = 0.0;
     if (dal[n] * dar[n] > 0.0) {
-      const double lim_slope1 = rmin(fabs(dal[n]), fabs(dar[n]));
-      const double lim_slope2 = rmin(0.5 * fabs(dac[n]), fabs(dag[n]));
+      const T lim_slope1 = rmin(fabs(dal[n]), fabs(dar[n]));
+      const T lim_slope2 = rmin(0.5 * fabs(dac[n]), fabs(dag[n]));
       da[n] = rsign(dac[n]) * rmin(2.0 * lim_slope1, lim_slope2);
     }
   }
 
   // Step 5: back to primitive slopes, dWm[n] = sum_m da[m]*R[n][m].
-  double dWm[7];
+  T dWm[7];
   dWm[0] = da[0] * E.R00 + da[2] * E.R02 + da[3] + da[4] * E.R02 + da[6] * E.R00;
   dWm[1] = da[0] * E.R10 + da[2] * E.R12 + da[4] * -E.R12 + da[6] * -E.R10;
   dWm[2] = da[0] * E.R20 + da[1] * E.R21 + da[2] * E.R22 + da[4] * -E.R22 + da[5] * -E.R21 + da[6] * -E.R20;
@@ -283,11 +296,11 @@ ATHB_HD void plm_cell(const Prim1& wm, const Prim1& w0, const Prim1& wp, double 
   dWm[6] = da[0] * E.R60 + da[1] * E.R61 + da[2] * E.R62 + da[4] * E.R62 + da[5] * E.R61 + da[6] * E.R60;
 
   // Step 7: L/R values, bounded by the neighbouring cell centres.
-  double Wlv[7], Wrv[7], dW[7];
+  T Wlv[7], Wrv[7], dW[7];
 #pragma unroll
   for (int n = 0; n < 7; n++) {
-    double l = W0[n] - 0.5 * dWm[n];
-    double r = W0[n] + 0.5 * dWm[n];
+    T l = W0[n] - 0.5 * dWm[n];
+    T r = W0[n] + 0.5 * dWm[n];
     l = rmax(rmin(W0[n], Wm[n]), l);
     l = rmin(rmax(W0[n], Wm[n]), l);
     r = rmax(rmin(W0[n], Wp[n]), r);
@@ -298,12 +311,12 @@ ATHB_HD void plm_cell(const Prim1& wm, const Prim1& w0, const Prim1& wp, double 
   }
 
   // Step 8: integrate over the domain of dependence of the extreme waves.
-  double pWl[7], pWr[7];
+  T pWl[7], pWr[7];
   {
-    const double qx = 0.5 * rmax(E.ev[6], 0.0) * dtodx;
+    const T qx = 0.5 * rmax(E.ev[6], T(0.0)) * dtodx;
 #pragma unroll
     for (int n = 0; n < 7; n++) pWl[n] = Wrv[n] - qx * dW[n];
-    const double qy = -0.5 * rmin(E.ev[0], 0.0) * dtodx;
+    const T qy = -0.5 * rmin(E.ev[0], T(0.0)) * dtodx;
 #pragma unroll
     for (int n = 0; n < 7; n++) pWr[n] = Wlv[n] + qy * dW[n];
   }
@@ -314,15 +327,15 @@ ATHB_HD void plm_cell(const Prim1& wm, const Prim1& w0, const Prim1& wp, double 
 #pragma unroll
   for (int n = 0; n < 6; n++) {
     if (E.ev[n] > 0.) {
-      double l[7], r[7];
+      T l[7], r[7];
       prim_left_row(E, n, l);
-      const double dev = E.ev[6] - E.ev[n];
-      double qa = 0.0;
+      const T dev = E.ev[6] - E.ev[n];
+      T qa = T(0.0);
       bool first = true;
 #pragma unroll
       for (int m = 0; m < 7; m++) {
         if (!((prim_left_mask(n) >> m) & 1)) continue;
-        const double t = l[m] * 0.5 * dtodx * dev * dW[m];
+        const T t = l[m] * 0.5 * dtodx * dev * dW[m];
         qa = first ? t : qa + t;
         first = false;
       }
@@ -335,19 +348,19 @@ ATHB_HD void plm_cell(const Prim1& wm, const Prim1& w0, const Prim1& wp, double 
 #pragma unroll
   for (int n = 0; n < 7; n++) {
     if (E.ev[n] < 0.) {
-      double l[7], r[7], h[7];
+      T l[7], r[7], h[7];
       prim_left_row(E, n, l);
       prim_right_col(E, n, r);
 #pragma unroll
       for (int m = 0; m < 7; m++) h[m] = l[m] * 0.5 * dtodx;
       if (n != 0) {
-        const double dev = E.ev[0] - E.ev[n];
-        double qa = 0.0;
+        const T dev = E.ev[0] - E.ev[n];
+        T qa = T(0.0);
         bool first = true;
 #pragma unroll
         for (int m = 0; m < 7; m++) {
           if (!((prim_left_mask(n) >> m) & 1)) continue;
-          const double t = h[m] * dev * dW[m];
+          const T t = h[m] * dev * dW[m];
           qa = first ? t : qa + t;
           first = false;
         }
@@ -356,13 +369,13 @@ ATHB_HD void plm_cell(const Prim1& wm, const Prim1& w0, const Prim1& wp, double 
           if ((prim_right_mask(n) >> m) & 1) pWr[m] += qa * r[m];
       }
       {
-        const double dev = E.ev[n] - E.ev[6];
-        double qa = 0.0;
+        const T dev = E.ev[n] - E.ev[6];
+        T qa = T(0.0);
         bool first = true;
 #pragma unroll
         for (int m = 0; m < 7; m++) {
           if (!((prim_left_mask(n) >> m) & 1)) continue;
-          const double t = h[m] * dev * dW[m];
+          const T t = h[m] * dev * dW[m];
           qa = first ? t : qa + t;
           first = false;
         }
@@ -383,13 +396,15 @@ ATHB_HD void plm_cell(const Prim1& wm, const Prim1& w0, const Prim1& wp, double 
 // Roe-averaged state shared by the Roe and HLLE solvers
 // (src/flux_roe.c:91-114, src/flux_hlle.c:87-110).
 // ---------------------------------------------------------------------------
-struct RoeAvg {
-  double sqrtdl, sqrtdr, isdlpdr, droe, v1, v2, v3, b2, b3, x, y, pbl, pbr, h;
+template <class T> struct RoeAvgT {
+  T sqrtdl, sqrtdr, isdlpdr, droe, v1, v2, v3, b2, b3, x, y, pbl, pbr, h;
 };
+using RoeAvg = RoeAvgT<double>;
 
-ATHB_HD RoeAvg roe_average(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const Prim1& Wr,
-                           double Bxi) {
-  RoeAvg r;
+template <class T>
+ATHB_HD RoeAvgT<T> roe_average(const Cons1T<T>& Ul, const Cons1T<T>& Ur, const Prim1T<T>& Wl, const Prim1T<T>& Wr,
+                           T Bxi) {
+  RoeAvgT<T> r;
   r.sqrtdl = sqrt(Wl.d);
   r.sqrtdr = sqrt(Wr.d);
   r.isdlpdr = 1.0 / (r.sqrtdl + r.sqrtdr);
@@ -399,7 +414,7 @@ ATHB_HD RoeAvg roe_average(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, co
   r.v3 = (r.sqrtdl * Wl.vz + r.sqrtdr * Wr.vz) * r.isdlpdr;
   r.b2 = (r.sqrtdr * Wl.by + r.sqrtdl * Wr.by) * r.isdlpdr;
   r.b3 = (r.sqrtdr * Wl.bz + r.sqrtdl * Wr.bz) * r.isdlpdr;
-  const double dby = Wl.by - Wr.by, dbz = Wl.bz - Wr.bz, ss = r.sqrtdl + r.sqrtdr;
+  const T dby = Wl.by - Wr.by, dbz = Wl.bz - Wr.bz, ss = r.sqrtdl + r.sqrtdr;
   r.x = 0.5 * (dby * dby + dbz * dbz) / (ss * ss);
   r.y = 0.5 * (Wl.d + Wr.d) / r.droe;
   r.pbl = 0.5 * (Bxi * Bxi + Wl.by * Wl.by + Wl.bz * Wl.bz);
@@ -409,12 +424,14 @@ ATHB_HD RoeAvg roe_average(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, co
 }
 
 // Roe-matrix wave speeds (src/esystem_roe.c:68-87,136-144).
-struct RoeSpeeds {
-  double di, vsq, btsq, bt_starsq, vaxsq, hp, twid_asq, cfsq, cf, cssq, cs, vax, gfac;
+template <class T> struct RoeSpeedsT {
+  T di, vsq, btsq, bt_starsq, vaxsq, hp, twid_asq, cfsq, cf, cssq, cs, vax, gfac;
 };
+using RoeSpeeds = RoeSpeedsT<double>;
 
-ATHB_HD RoeSpeeds roe_speeds(const RoeAvg& r, double b1, const Eos& eos) {
-  RoeSpeeds s;
+template <class T>
+ATHB_HD RoeSpeedsT<T> roe_speeds(const RoeAvgT<T>& r, T b1, const Eos& eos) {
+  RoeSpeedsT<T> s;
   s.di = 1.0 / r.droe;
   s.vsq = r.v1 * r.v1 + r.v2 * r.v2 + r.v3 * r.v3;
   s.btsq = r.b2 * r.b2 + r.b3 * r.b3;
@@ -422,11 +439,11 @@ ATHB_HD RoeSpeeds roe_speeds(const RoeAvg& r, double b1, const Eos& eos) {
   s.bt_starsq = s.gfac * s.btsq;
   s.vaxsq = b1 * b1 * s.di;
   s.hp = r.h - (s.vaxsq + s.btsq * s.di);
-  s.twid_asq = rmax((eos.gamma_1 * (s.hp - 0.5 * s.vsq) - eos.gamma_2 * r.x), kTiny);
-  const double ct2 = s.bt_starsq * s.di;
-  const double tsum = s.vaxsq + ct2 + s.twid_asq;
-  const double tdif = s.vaxsq + ct2 - s.twid_asq;
-  const double cf2_cs2 = sqrt(tdif * tdif + 4.0 * s.twid_asq * ct2);
+  s.twid_asq = rmax((eos.gamma_1 * (s.hp - 0.5 * s.vsq) - eos.gamma_2 * r.x), T(kTiny));
+  const T ct2 = s.bt_starsq * s.di;
+  const T tsum = s.vaxsq + ct2 + s.twid_asq;
+  const T tdif = s.vaxsq + ct2 - s.twid_asq;
+  const T cf2_cs2 = sqrt(tdif * tdif + 4.0 * s.twid_asq * ct2);
   s.cfsq = 0.5 * (tsum + cf2_cs2);
   s.cf = sqrt(s.cfsq);
   s.cssq = s.twid_asq * s.vaxsq / s.cfsq;
@@ -448,29 +465,31 @@ ATHB_HD RoeSpeeds roe_speeds(const RoeAvg& r, double b1, const Eos& eos) {
 //     c6 = (af, af*ev6, af*v2-qs*b2*, af*v3-qs*b3*, R46, as'*b2*, as'*b3*)
 //   L rows: row 5 = (-L10, 0, -L12, -L13, 0, L15, L16) of row 1; rows 2/4 and
 //   0/6 share their last three entries.
-struct RoeScal {
-  double v1, v2, v3, b2, b3, vsq, hp, cf, cs;
-  double af, as, qf, qs;            // alpha_f, alpha_s, qf, qs (right vectors)
-  double bet2, bet3, bet2s, bet3s, vbet, aspbb, afpbb, sgn, isqrtd, sqrtd, asp, afp, gx;
-  double afn, asn, cff, css, qfn, qsn, Afn, Asn, afpb, aspb, q2s, q3s, vqstr, norm2;  // left vectors
+template <class T> struct RoeScalT {
+  T v1, v2, v3, b2, b3, vsq, hp, cf, cs;
+  T af, as, qf, qs;            // alpha_f, alpha_s, qf, qs (right vectors)
+  T bet2, bet3, bet2s, bet3s, vbet, aspbb, afpbb, sgn, isqrtd, sqrtd, asp, afp, gx;
+  T afn, asn, cff, css, qfn, qsn, Afn, Asn, afpb, aspb, q2s, q3s, vqstr, norm2;  // left vectors
 };
+using RoeScal = RoeScalT<double>;
 
-ATHB_HD void roe_scalars(const RoeAvg& r, const RoeSpeeds& s, double b1, const Eos& eos, RoeScal& S) {
-  const double v2 = r.v2, v3 = r.v3, b2 = r.b2, b3 = r.b3, d = r.droe;
+template <class T>
+ATHB_HD void roe_scalars(const RoeAvgT<T>& r, const RoeSpeedsT<T>& s, T b1, const Eos& eos, RoeScalT<T>& S) {
+  const T v2 = r.v2, v3 = r.v3, b2 = r.b2, b3 = r.b3, d = r.droe;
   S.v1 = r.v1; S.v2 = v2; S.v3 = v3; S.b2 = b2; S.b3 = b3;
   S.vsq = s.vsq; S.hp = s.hp; S.cf = s.cf; S.cs = s.cs;
-  const double bt = sqrt(s.btsq);
-  const double bt_star = sqrt(s.bt_starsq);
-  double bet2, bet3;
+  const T bt = sqrt(s.btsq);
+  const T bt_star = sqrt(s.bt_starsq);
+  T bet2, bet3;
   if (bt == 0.0) { bet2 = 1.0; bet3 = 0.0; } else { bet2 = b2 / bt; bet3 = b3 / bt; }
-  const double sg = sqrt(s.gfac);
-  const double bet2_star = bet2 / sg;
-  const double bet3_star = bet3 / sg;
-  const double bet_starsq = bet2_star * bet2_star + bet3_star * bet3_star;
+  const T sg = sqrt(s.gfac);
+  const T bet2_star = bet2 / sg;
+  const T bet3_star = bet3 / sg;
+  const T bet_starsq = bet2_star * bet2_star + bet3_star * bet3_star;
   S.bet2 = bet2; S.bet3 = bet3; S.bet2s = bet2_star; S.bet3s = bet3_star;
   S.vbet = v2 * bet2_star + v3 * bet3_star;
 
-  double alpha_f, alpha_s;
+  T alpha_f, alpha_s;
   if ((s.cfsq - s.cssq) == 0.0) { alpha_f = 1.0; alpha_s = 0.0; }
   else if ((s.twid_asq - s.cssq) <= 0.0) { alpha_f = 0.0; alpha_s = 1.0; }
   else if ((s.cfsq - s.twid_asq) <= 0.0) { alpha_f = 1.0; alpha_s = 0.0; }
@@ -478,21 +497,21 @@ ATHB_HD void roe_scalars(const RoeAvg& r, const RoeSpeeds& s, double b1, const E
     alpha_f = sqrt((s.twid_asq - s.cssq) / (s.cfsq - s.cssq));
     alpha_s = sqrt((s.cfsq - s.twid_asq) / (s.cfsq - s.cssq));
   }
-  const double sqrtd = sqrt(d);
-  const double isqrtd = 1.0 / sqrtd;
-  const double sgn = rsign(b1);
-  const double twid_a = sqrt(s.twid_asq);
-  const double qf = s.cf * alpha_f * sgn;
-  const double qs = s.cs * alpha_s * sgn;
-  const double af_prime = twid_a * alpha_f * isqrtd;
-  const double as_prime = twid_a * alpha_s * isqrtd;
+  const T sqrtd = sqrt(d);
+  const T isqrtd = 1.0 / sqrtd;
+  const T sgn = rsign(b1);
+  const T twid_a = sqrt(s.twid_asq);
+  const T qf = s.cf * alpha_f * sgn;
+  const T qs = s.cs * alpha_s * sgn;
+  const T af_prime = twid_a * alpha_f * isqrtd;
+  const T as_prime = twid_a * alpha_s * isqrtd;
   S.af = alpha_f; S.as = alpha_s; S.qf = qf; S.qs = qs;
   S.afpbb = af_prime * bt_star * bet_starsq;
   S.aspbb = as_prime * bt_star * bet_starsq;
   S.sgn = sgn; S.isqrtd = isqrtd; S.sqrtd = sqrtd; S.asp = as_prime; S.afp = af_prime;
   S.gx = eos.gamma_2 * r.x / eos.gamma_1;
 
-  double norm = 0.5 / s.twid_asq;
+  T norm = 0.5 / s.twid_asq;
   S.cff = norm * alpha_f * s.cf;
   S.css = norm * alpha_s * s.cs;
   S.qfn = qf * norm;
@@ -511,7 +530,8 @@ ATHB_HD void roe_scalars(const RoeAvg& r, const RoeSpeeds& s, double b1, const E
 }
 
 // Column n of the Roe right-eigenmatrix.
-ATHB_HD void roe_right_col(const RoeScal& S, const double ev[7], int n, double c[7]) {
+template <class T>
+ATHB_HD void roe_right_col(const RoeScalT<T>& S, const T ev[7], int n, T c[7]) {
   switch (n) {
   case 0:
     c[0] = S.af; c[1] = S.af * ev[0]; c[2] = S.af * S.v2 + S.qs * S.bet2s; c[3] = S.af * S.v3 + S.qs * S.bet3s;
@@ -545,12 +565,13 @@ ATHB_HD int roe_right_mask(int n) {  // structural non-zeros of column n
 
 // a = L * dU (src/flux_roe.c:200-204), terms in column order, zeros skipped,
 // rows formed in pairs that share entries.
-ATHB_HD void roe_project(const RoeScal& S, const double u[7], double a[7]) {
-  const double vh = S.vsq - S.hp;
+template <class T>
+ATHB_HD void roe_project(const RoeScalT<T>& S, const T u[7], T a[7]) {
+  const T vh = S.vsq - S.hp;
   {  // rows 0 and 6
-    const double p4 = S.afn * u[4];
-    const double p5 = (S.Asn * S.q2s - S.afn * S.b2) * u[5];
-    const double p6 = (S.Asn * S.q3s - S.afn * S.b3) * u[6];
+    const T p4 = S.afn * u[4];
+    const T p5 = (S.Asn * S.q2s - S.afn * S.b2) * u[5];
+    const T p6 = (S.Asn * S.q3s - S.afn * S.b3) * u[6];
     a[0] = (S.afn * vh + S.cff * (S.cf + S.v1) - S.qsn * S.vqstr - S.aspb) * u[0] +
            (-S.afn * S.v1 - S.cff) * u[1] + (-S.afn * S.v2 + S.qsn * S.q2s) * u[2] +
            (-S.afn * S.v3 + S.qsn * S.q3s) * u[3] + p4 + p5 + p6;
@@ -559,18 +580,18 @@ ATHB_HD void roe_project(const RoeScal& S, const double u[7], double a[7]) {
            (-S.afn * S.v3 - S.qsn * S.q3s) * u[3] + p4 + p5 + p6;
   }
   {  // rows 1 and 5
-    const double p0 = (0.5 * (S.v2 * S.bet3 - S.v3 * S.bet2)) * u[0];
-    const double p2 = (-0.5 * S.bet3) * u[2];
-    const double p3 = (0.5 * S.bet2) * u[3];
-    const double p5 = (-0.5 * S.sqrtd * S.bet3 * S.sgn) * u[5];
-    const double p6 = (0.5 * S.sqrtd * S.bet2 * S.sgn) * u[6];
+    const T p0 = (0.5 * (S.v2 * S.bet3 - S.v3 * S.bet2)) * u[0];
+    const T p2 = (-0.5 * S.bet3) * u[2];
+    const T p3 = (0.5 * S.bet2) * u[3];
+    const T p5 = (-0.5 * S.sqrtd * S.bet3 * S.sgn) * u[5];
+    const T p6 = (0.5 * S.sqrtd * S.bet2 * S.sgn) * u[6];
     a[1] = p0 + p2 + p3 + p5 + p6;
     a[5] = -p0 - p2 - p3 + p5 + p6;
   }
   {  // rows 2 and 4
-    const double p4 = S.asn * u[4];
-    const double p5 = (-S.Afn * S.q2s - S.asn * S.b2) * u[5];
-    const double p6 = (-S.Afn * S.q3s - S.asn * S.b3) * u[6];
+    const T p4 = S.asn * u[4];
+    const T p5 = (-S.Afn * S.q2s - S.asn * S.b2) * u[5];
+    const T p6 = (-S.Afn * S.q3s - S.asn * S.b3) * u[6];
     a[2] = (S.asn * vh + S.css * (S.cs + S.v1) + S.qfn * S.vqstr + S.afpb) * u[0] +
            (-S.asn * S.v1 - S.css) * u[1] + (-S.asn * S.v2 - S.qfn * S.q2s) * u[2] +
            (-S.asn * S.v3 - S.qfn * S.q3s) * u[3] + p4 + p5 + p6;
@@ -585,8 +606,9 @@ ATHB_HD void roe_project(const RoeScal& S, const double u[7], double a[7]) {
 }
 
 // Physical flux of one side (src/flux_roe.c:136-172).
-ATHB_HD Cons1 side_flux(const Cons1& U, const Prim1& W, double Bxi, double pb) {
-  Cons1 F;
+template <class T>
+ATHB_HD Cons1T<T> side_flux(const Cons1T<T>& U, const Prim1T<T>& W, T Bxi, T pb) {
+  Cons1T<T> F;
   F.d = U.mx;
   F.mx = U.mx * W.vx;
   F.my = U.mx * W.vy;
@@ -603,19 +625,20 @@ ATHB_HD Cons1 side_flux(const Cons1& U, const Prim1& W, double Bxi, double pb) {
 }
 
 // --- src/flux_hlle.c:60-199 ---------------------------------------------------
-ATHB_HD Cons1 flux_hlle(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const Prim1& Wr,
-                        double Bxi, const Eos& eos) {
-  const RoeAvg r = roe_average(Ul, Ur, Wl, Wr, Bxi);
-  const RoeSpeeds s = roe_speeds(r, Bxi, eos);
-  const double ev0 = r.v1 - s.cf, ev6 = r.v1 + s.cf;
+template <class T>
+ATHB_HD Cons1T<T> flux_hlle(const Cons1T<T>& Ul, const Cons1T<T>& Ur, const Prim1T<T>& Wl, const Prim1T<T>& Wr,
+                        T Bxi, const Eos& eos) {
+  const RoeAvgT<T> r = roe_average(Ul, Ur, Wl, Wr, Bxi);
+  const RoeSpeedsT<T> s = roe_speeds(r, Bxi, eos);
+  const T ev0 = r.v1 - s.cf, ev6 = r.v1 + s.cf;
 
-  double asq = eos.gamma * Wl.p / Wl.d;
-  double vaxsq = Bxi * Bxi / Wl.d;
-  double ct2 = (Ul.by * Ul.by + Ul.bz * Ul.bz) / Wl.d;
-  double qsq = vaxsq + ct2 + asq;
-  double tmp = vaxsq + ct2 - asq;
-  double cfsq = 0.5 * (qsq + sqrt(tmp * tmp + 4.0 * asq * ct2));
-  const double cfl = sqrt(cfsq);
+  T asq = eos.gamma * Wl.p / Wl.d;
+  T vaxsq = Bxi * Bxi / Wl.d;
+  T ct2 = (Ul.by * Ul.by + Ul.bz * Ul.bz) / Wl.d;
+  T qsq = vaxsq + ct2 + asq;
+  T tmp = vaxsq + ct2 - asq;
+  T cfsq = 0.5 * (qsq + sqrt(tmp * tmp + 4.0 * asq * ct2));
+  const T cfl = sqrt(cfsq);
 
   asq = eos.gamma * Wr.p / Wr.d;
   vaxsq = Bxi * Bxi / Wr.d;
@@ -623,14 +646,14 @@ ATHB_HD Cons1 flux_hlle(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const
   qsq = vaxsq + ct2 + asq;
   tmp = vaxsq + ct2 - asq;
   cfsq = 0.5 * (qsq + sqrt(tmp * tmp + 4.0 * asq * ct2));
-  const double cfr = sqrt(cfsq);
+  const T cfr = sqrt(cfsq);
 
-  const double ar = rmax(ev6, (Wr.vx + cfr));
-  const double al = rmin(ev0, (Wl.vx - cfl));
-  const double bp = rmax(ar, 0.0);
-  const double bm = rmin(al, 0.0);
+  const T ar = rmax(ev6, (Wr.vx + cfr));
+  const T al = rmin(ev0, (Wl.vx - cfl));
+  const T bp = rmax(ar, T(0.0));
+  const T bm = rmin(al, T(0.0));
 
-  Cons1 Fl, Fr;
+  Cons1T<T> Fl, Fr;
   Fl.d = Ul.mx - bm * Ul.d;
   Fr.d = Ur.mx - bp * Ur.d;
   Fl.mx = Ul.mx * (Wl.vx - bm);
@@ -656,8 +679,8 @@ ATHB_HD Cons1 flux_hlle(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const
   Fl.bz = Wl.bz * (Wl.vx - bm) - Bxi * Wl.vz;
   Fr.bz = Wr.bz * (Wr.vx - bp) - Bxi * Wr.vz;
 
-  const double t = 0.5 * (bp + bm) / (bp - bm);
-  Cons1 F;
+  const T t = 0.5 * (bp + bm) / (bp - bm);
+  Cons1T<T> F;
   F.d = 0.5 * (Fl.d + Fr.d) + (Fl.d - Fr.d) * t;
   F.mx = 0.5 * (Fl.mx + Fr.mx) + (Fl.mx - Fr.mx) * t;
   F.my = 0.5 * (Fl.my + Fr.my) + (Fl.my - Fr.my) * t;
@@ -669,11 +692,12 @@ ATHB_HD Cons1 flux_hlle(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const
 }
 
 // --- src/flux_roe.c:54-259 ----------------------------------------------------
-ATHB_HD Cons1 flux_roe(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const Prim1& Wr,
-                       double Bxi, const Eos& eos) {
-  const RoeAvg r = roe_average(Ul, Ur, Wl, Wr, Bxi);
-  const RoeSpeeds s = roe_speeds(r, Bxi, eos);
-  double ev[7];
+template <class T>
+ATHB_HD Cons1T<T> flux_roe(const Cons1T<T>& Ul, const Cons1T<T>& Ur, const Prim1T<T>& Wl, const Prim1T<T>& Wr,
+                       T Bxi, const Eos& eos) {
+  const RoeAvgT<T> r = roe_average(Ul, Ur, Wl, Wr, Bxi);
+  const RoeSpeedsT<T> s = roe_speeds(r, Bxi, eos);
+  T ev[7];
   ev[0] = r.v1 - s.cf; ev[1] = r.v1 - s.vax; ev[2] = r.v1 - s.cs; ev[3] = r.v1;
   ev[4] = r.v1 + s.cs; ev[5] = r.v1 + s.vax; ev[6] = r.v1 + s.cf;
 
@@ -681,21 +705,21 @@ ATHB_HD Cons1 flux_roe(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const 
   if (ev[0] >= 0.0) return side_flux(Ul, Wl, Bxi, r.pbl);
   if (ev[6] <= 0.0) return side_flux(Ur, Wr, Bxi, r.pbr);
 
-  RoeScal S;
+  RoeScalT<T> S;
   roe_scalars(r, s, Bxi, eos, S);
 
   // Step 6: wave strengths.
-  double a[7];
+  T a[7];
   {
-    const double dU[7] = {Ur.d - Ul.d, Ur.mx - Ul.mx, Ur.my - Ul.my, Ur.mz - Ul.mz,
+    const T dU[7] = {Ur.d - Ul.d, Ur.mx - Ul.mx, Ur.my - Ul.my, Ur.mz - Ul.mz,
                           Ur.e - Ul.e, Ur.by - Ul.by, Ur.bz - Ul.bz};
     roe_project(S, dU, a);
   }
   // Step 8 starts from the mean of the side fluxes (src/flux_roe.c:252)
-  double F[7];
+  T F[7];
   {
-    const Cons1 Fl = side_flux(Ul, Wl, Bxi, r.pbl);
-    const Cons1 Fr = side_flux(Ur, Wr, Bxi, r.pbr);
+    const Cons1T<T> Fl = side_flux(Ul, Wl, Bxi, r.pbl);
+    const Cons1T<T> Fr = side_flux(Ur, Wr, Bxi, r.pbr);
     F[0] = 0.5 * (Fl.d + Fr.d); F[1] = 0.5 * (Fl.mx + Fr.mx); F[2] = 0.5 * (Fl.my + Fr.my);
     F[3] = 0.5 * (Fl.mz + Fr.mz); F[4] = 0.5 * (Fl.e + Fr.e); F[5] = 0.5 * (Fl.by + Fr.by);
     F[6] = 0.5 * (Fl.bz + Fr.bz);
@@ -703,10 +727,10 @@ ATHB_HD Cons1 flux_roe(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const 
   // Steps 7 and 8 fused over the right eigenvectors: the intermediate states
   // (positivity test, HLLE on failure) and the Roe flux subtract the same
   // column n; per component the flux terms keep the reference's order.
-  double u[7] = {Ul.d, Ul.mx, Ul.my, Ul.mz, Ul.e, Ul.by, Ul.bz};
+  T u[7] = {Ul.d, Ul.mx, Ul.my, Ul.mz, Ul.e, Ul.by, Ul.bz};
 #pragma unroll
   for (int n = 0; n < 7; n++) {
-    double c[7];
+    T c[7];
     roe_right_col(S, ev, n, c);
     if (n < 6) {
 #pragma unroll
@@ -715,19 +739,19 @@ ATHB_HD Cons1 flux_roe(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const 
       if (ev[n + 1] > ev[n]) {
         bool bad = (u[0] <= 0.0);
         if (!bad) {
-          double p_inter = u[4] - 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0];
+          T p_inter = u[4] - 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0];
           p_inter -= 0.5 * (u[5] * u[5] + u[6] * u[6] + Bxi * Bxi);
           bad = (p_inter < 0.0);
         }
         if (bad) return flux_hlle(Ul, Ur, Wl, Wr, Bxi, eos);
       }
     }
-    const double coeff = 0.5 * rmax(fabs(ev[n]), 0.0) * a[n];
+    const T coeff = 0.5 * rmax(fabs(ev[n]), T(0.0)) * a[n];
 #pragma unroll
     for (int k = 0; k < 7; k++)
       if ((roe_right_mask(n) >> k) & 1) F[k] -= coeff * c[k];
   }
-  Cons1 out;
+  Cons1T<T> out;
   out.d = F[0]; out.mx = F[1]; out.my = F[2]; out.mz = F[3]; out.e = F[4]; out.by = F[5]; out.bz = F[6];
   return out;
 }
@@ -736,9 +760,9 @@ ATHB_HD Cons1 flux_roe(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const 
 // 238,444,461); HLLE everywhere is the optional alternative.
 enum FluxKind { kFluxRoe = 0, kFluxHlle = 1 };
 
-template <int FLUX>
-ATHB_HD Cons1 riemann(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const Prim1& Wr,
-                      double Bxi, const Eos& eos) {
+template <int FLUX, class T>
+ATHB_HD Cons1T<T> riemann(const Cons1T<T>& Ul, const Cons1T<T>& Ur, const Prim1T<T>& Wl, const Prim1T<T>& Wr,
+                          T Bxi, const Eos& eos) {
   if (FLUX == kFluxHlle) return flux_hlle(Ul, Ur, Wl, Wr, Bxi, eos);
   return flux_roe(Ul, Ur, Wl, Wr, Bxi, eos);
 }

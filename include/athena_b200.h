@@ -286,6 +286,10 @@ int athb_batch_timing(athb_batch *b, int enable, double *ms_out);
 #define ATHB_BATCH_PHASED 1
 int athb_batch_set_mode(athb_batch *b, int mode);
 int athb_batch_mode(const athb_batch *b);
+/* A grid barrier that times out in the persistent kernel (a block that never
+ * arrived) sets a sticky ATHB_ERR_STATE on the batch and leaves the barrier's
+ * arrival count inconsistent: every later athb_batch_run on that batch
+ * reports the time-out again.  Destroy the batch and create a new one.      */
 /* Failure-path self-test of the persistent kernel's grid barrier: one block
  * waits for two, gives up after `spins` polls (~64 ns each), and the time-out
  * is reported in *timed_out (1 expected) with the device still usable.      */
@@ -306,7 +310,9 @@ int athb_batch_selftest_barrier(int device, long long spins, int *timed_out);
  * ATHB_ERR_ARG.  All calls share that array: calls that overlap on the GPU
  * race.  The array's device address is looked up on the first call made on
  * each device (that device current); make that first call before any stream
- * capture.                                                                  */
+ * capture.  The step runs on the calling thread's current device, which must
+ * be cfg->device (ATHB_ERR_ARG otherwise).  It does no non-finite check: a
+ * step that produces NaN or a negative pressure returns ATHB_OK.            */
 int athb_integrate_noalloc(const athb_config *cfg, const double *d_in, double *d_out, double dt,
                            void *stream);
 

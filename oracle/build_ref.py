@@ -7,7 +7,9 @@ binaries go to ``oracle/_ref/`` (git-ignored; it still travels to GPU boxes).
 
 Builds, per problem generator and flux:
 
-* ``athref_{blast,field_loop,cpaw2d,file}_{roe,hlle}``: the reference CPU step.
+* ``athref_{blast,field_loop,cpaw2d,file,userbc}_{roe,hlle}``: the reference CPU
+  step (``userbc``: oracle/userbc_problem.c, a user boundary condition set
+  through ``set_bvals_fun``).
   ``roe`` is the reference as shipped (``__integrate_2d__.c`` always calls
   ``flux_roe``, ``__integrate_2d__.c:178,238,444,461``); ``hlle`` recompiles
   ``__integrate_2d__.c`` alone with ``-Dflux_roe=flux_hlle``.
@@ -26,7 +28,9 @@ Flags: ``-O2 -ffp-contract=off`` (no FMA contraction, so every ``+ - * /`` and
 are ``-O0 -mpc64`` (src/Debug/subdir.mk:130); ``-mpc64`` only affects x87 and
 x86-64 uses SSE2 for double, so results are identical; ``-O0`` is ~3x slower.
 
-Usage: ``python oracle/build_ref.py [--ref <reference root>] [--force]``.
+Usage: ``python oracle/build_ref.py [--ref <reference root>] [--force]``; the
+reference root defaults to ``$ATHENA_REF``, else ``../reference`` beside the
+repository.
 """
 from __future__ import annotations
 
@@ -38,7 +42,16 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-DEFAULT_REF = Path("/root/reference")
+
+
+def default_reference() -> Path:
+    """The reference checkout: $ATHENA_REF, else a ``reference`` directory
+    beside this repository."""
+    env = os.environ.get("ATHENA_REF")
+    return Path(env) if env else HERE.parent.parent / "reference"
+
+
+DEFAULT_REF = default_reference()
 
 # Reference CPU sources on the step path (plus host glue they need to link).
 CORE = [
@@ -54,6 +67,9 @@ PROBLEMS = {
     "field_loop": ("field_loop.c", []),  # FIELD_LOOP is defined by debug_tools_cuda.h:73
     "cpaw2d": ("cpaw2d.c", ["-DCPAW2D"]),
     "file": (None, ["-DHARNESS_FILE_PROBLEM"]),
+    # a user boundary condition registered through set_bvals_fun (test problem
+    # of this directory, not a reference file)
+    "userbc": (HERE / "userbc_problem.c", []),
 }
 # The reference's main program and its output path (athmain_*).
 MAIN_EXTRA = [
@@ -103,14 +119,14 @@ def build(ref_root: Path = DEFAULT_REF, force: bool = False, lib: Path | None = 
     built = []
     for prob, (pfile, pdefs) in PROBLEMS.items():
         harness = _cc(HERE / "ref_harness.c", obj / f"harness_{prob}.o", pdefs, inc, force)
-        pobj = [] if pfile is None else [_cc(src / pfile, obj / f"prob_{prob}.o", pdefs, inc, force)]
+        pobj = [] if pfile is None else [_cc(src / pfile, obj / f"prob_{prob}.o", pdefs, inc, force)]  # src / absolute = absolute
         for flux, iobj in integ.items():
             exe = OUT / f"athref_{prob}_{flux}"
             deps = [harness, iobj, *core, *pobj]
             if force or not _newer(exe, deps):
                 _run(["gcc", "-o", str(exe), *map(str, deps), *LDCUDA, "-lm"])
             built.append(exe)
-        if pfile is not None:
+        if pfile is not None and not Path(pfile).is_absolute():
             mobj = [_cc(src / f, obj / f"main_{prob}_{f[:-2]}.o", pdefs, inc, force) for f in MAIN_EXTRA]
             stub = _cc(HERE / "ref_stubs.c", obj / "ref_stubs.o", [], inc, force)
             exe = OUT / f"athmain_{prob}"

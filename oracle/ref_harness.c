@@ -22,6 +22,9 @@
  *               appends the L1 errors to ./cpaw2d-errors.dat
  *   --bench     print one JSON line with the main-loop time (zone-cycles/s)
  *   --max-seconds T  also stop once the main loop has run for T seconds
+ *   --warmup N  run N untimed iterations before the timed loop (--steps
+ *               counts the timed ones); --warmup-seconds T stops the
+ *               warm-up once it has run for T seconds
  *
  * Raw state file format (little endian):
  *   int32  magic 0x41544842 ("ATHB"), version 1
@@ -123,6 +126,8 @@ int main(int argc, char **argv)
   long steps = -1;
   int want_l1 = 0, bench = 0;
   double max_seconds = -1.0;
+  long warmup = 0;
+  double warmup_seconds = -1.0;
   Grid G;
   memset(&G, 0, sizeof(G));
 
@@ -134,6 +139,8 @@ int main(int argc, char **argv)
     else if (!strcmp(argv[a], "--l1")) want_l1 = 1;
     else if (!strcmp(argv[a], "--bench")) bench = 1;
     else if (!strcmp(argv[a], "--max-seconds") && a + 1 < argc) max_seconds = atof(argv[++a]);
+    else if (!strcmp(argv[a], "--warmup") && a + 1 < argc) warmup = atol(argv[++a]);
+    else if (!strcmp(argv[a], "--warmup-seconds") && a + 1 < argc) warmup_seconds = atof(argv[++a]);
     else if (!strcmp(argv[a], "--quiet")) ;
     else { fprintf(stderr, "unknown argument %s\n", argv[a]); return 2; }
   }
@@ -157,7 +164,19 @@ int main(int argc, char **argv)
   lr_states_init(G.Nx1, G.Nx2);
   integrate_init_2d(G.Nx1, G.Nx2);
 
-  /* src/main.c:221-318, without output */
+  /* src/main.c:221-318, without output: untimed warm-up iterations first */
+  long warm = 0;
+  double tw = now_s();
+  while (warm < warmup && G.time < tlim && (nlim < 0 || G.nstep < nlim)) {
+    if ((tlim - G.time) < G.dt) G.dt = (tlim - G.time);
+    integrate_2d(&G);
+    G.nstep++;
+    G.time += G.dt;
+    new_dt(&G);
+    set_bvals(&G, 0);
+    warm++;
+    if (warmup_seconds > 0.0 && now_s() - tw > warmup_seconds) break;
+  }
   double t0 = now_s();
   long done = 0;
   while (G.time < tlim && (nlim < 0 || G.nstep < nlim) && (steps < 0 || done < steps)) {
@@ -176,8 +195,8 @@ int main(int argc, char **argv)
   if (dump) dump_state(&G, dump);
   if (bench) {
     double zc = (double)G.Nx1 * (double)G.Nx2 * (double)done;
-    printf("{\"steps\": %ld, \"seconds\": %.6f, \"zone_cycles_per_s\": %.6e, "
-           "\"Nx1\": %d, \"Nx2\": %d}\n", done, t1 - t0,
+    printf("{\"steps\": %ld, \"warmup\": %ld, \"seconds\": %.6f, \"zone_cycles_per_s\": %.6e, "
+           "\"Nx1\": %d, \"Nx2\": %d}\n", done, warm, t1 - t0,
            (t1 > t0) ? zc / (t1 - t0) : 0.0, G.Nx1, G.Nx2);
   }
   lr_states_destruct();

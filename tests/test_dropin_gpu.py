@@ -26,6 +26,10 @@ CASES = {
     "blast_reflect_mixed": ("blast", configs.blast(30, 36, bc=(1, 4, 2, 1)), 15),
     "field_loop_64x32": ("field_loop", configs.field_loop(64, 32), 20),
     "cpaw2d_32x16_period": ("cpaw2d", configs.cpaw2d(32, 16), None),
+    # a user boundary condition registered by the problem file through
+    # set_bvals_fun (oracle/userbc_problem.c): inflow on the left x1 side
+    "userbc_inflow_40x30": ("userbc", configs.blast(40, 30, bc=(2, 2, 2, 2)), None),
+    "userbc_inflow_periodic_x2": ("userbc", configs.blast(36, 24, bc=(2, 2, 4, 4)), None),
 }
 
 

@@ -26,10 +26,15 @@ def _noalloc():
     return f
 
 
-def test_noalloc_step_matches_integrate_2d_twice(tmp_path):
+@pytest.mark.parametrize("nx1,nx2,bc", [
+    (40, 28, (4, 4, 4, 4)),   # (40+8)*(28+8) = 1728 cells; rows of 48 doubles
+    (30, 20, (2, 2, 1, 1)),   # rows of 38 doubles (not a multiple of 16), outflow / reflecting
+    (64, 64, (4, 4, 4, 4)),   # the largest grid the fixed scratch holds (72*72 = 5184 cells)
+])
+def test_noalloc_step_matches_integrate_2d_twice(nx1, nx2, bc, tmp_path):
     import torch
 
-    blocks = configs.blast(40, 28)  # (40+8)*(28+8) = 1728 cells, inside the fixed scratch
+    blocks = configs.blast(nx1, nx2, bc=bc)
     ath = write_athinput(tmp_path / "athinput", blocks)
     g = Grid.from_athinput(ath, "blast")  # problem, set_bvals, first new_dt
     planes, dt, _, _ = g.download()
@@ -70,6 +75,17 @@ def test_noalloc_rejects_grids_beyond_its_scratch(tmp_path):
     out = torch.zeros_like(buf)
     rc = _noalloc()(C.byref(cfg), buf.data_ptr(), out.data_ptr(), 1e-3, None)
     assert rc == 1 and b"5184" in lib().athb_last_error()
+
+
+def test_noalloc_rejects_a_config_for_another_device(tmp_path):
+    import torch
+
+    cfg = Params.from_blocks(configs.field_loop(16, 16)).config()
+    cfg.device = torch.cuda.current_device() + 1
+    buf = torch.zeros(11 * 24 * 24, dtype=torch.float64, device="cuda")
+    out = torch.zeros_like(buf)
+    rc = _noalloc()(C.byref(cfg), buf.data_ptr(), out.data_ptr(), 1e-3, None)
+    assert rc == 1 and b"current device" in lib().athb_last_error()
 
 
 def test_noalloc_writes_only_the_step_cells(tmp_path):
