@@ -38,6 +38,11 @@ class Config(C.Structure):
     ]
 
 
+class AdjointStats(C.Structure):
+    _fields_ = [("steps", C.c_int), ("snapshots", C.c_int), ("advances", C.c_longlong), ("taped", C.c_longlong),
+                ("workspace_bytes", C.c_longlong), ("seconds", C.c_double), ("tape_mode", C.c_int)]
+
+
 class GridInfo(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("nx1", "nx2", "sx", "sy", "is_", "ie", "js", "je")] + [
         (n, C.c_double) for n in ("dx1", "dx2", "x1_0", "x2_0")] + [
@@ -111,6 +116,8 @@ def lib() -> C.CDLL:
             "athb_diagnostics": (I, [P, dp]),
             "athb_get_ly": (I, [P]),
             "athb_host_free": (None, [P]),
+            "athb_tlm_run": (I, [P, I, dp, dp, dp, dp]),
+            "athb_adjoint_gradient": (I, [P, I, C.c_longlong, dp, dp, C.POINTER(AdjointStats)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -281,6 +288,30 @@ class Grid:
         out = np.zeros(6)
         _check(lib().athb_diagnostics(self._h, _dp(out)))
         return dict(zip(("mass", "energy", "emag", "bp2", "max_divb", "max_j3"), out.tolist()))
+
+    def tlm(self, nsteps: int, direction: np.ndarray, want_state: bool = False):
+        """Tangent-linear model of nsteps main-loop iterations from the
+        resident state (taken as the loop-entry state): (J, dJ[, dS^N]) for
+        J = sum over interior cells of (B1c^2 + B2c^2)/2 along `direction`
+        (host planes; ghost entries ignored).  The resident state is kept."""
+        d = np.ascontiguousarray(direction, dtype=np.float64)
+        assert d.shape == (NPLANES, self.sy, self.sx)
+        J, dJ = C.c_double(), C.c_double()
+        out = np.empty_like(d) if want_state else None
+        _check(lib().athb_tlm_run(self._h, nsteps, _dp(d), C.byref(J), C.byref(dJ),
+                                  _dp(out) if out is not None else None))
+        return (J.value, dJ.value, out) if want_state else (J.value, dJ.value)
+
+    def adjoint_gradient(self, nsteps: int, snapshot_bytes: int = 0):
+        """Adjoint of nsteps main-loop iterations from the resident state:
+        (J, dJ/d(state), stats).  snapshot_bytes bounds the device memory for
+        checkpoints (0: most of the free memory)."""
+        g = np.empty((NPLANES, self.sy, self.sx))
+        J = C.c_double()
+        st = AdjointStats()
+        _check(lib().athb_adjoint_gradient(self._h, nsteps, snapshot_bytes, C.byref(J), _dp(g), C.byref(st)))
+        stats = {k: getattr(st, k) for k, _ in AdjointStats._fields_}
+        return J.value, g, stats
 
     def cpaw2d_errors(self) -> np.ndarray:
         err = np.zeros(9)

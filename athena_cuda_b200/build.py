@@ -32,10 +32,11 @@ NVCC_FLAGS = ARCH + [
 CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", f"-I{ROOT / 'include'}",
              f"-I{CUDA_HOME / 'include'}"]
 
-CU_SOURCES = ["athb_core.cu", "athb_dropin.cu", "athb_batch.cu", "athb_noalloc.cu", "athb_output.cu",
+CU_SOURCES = ["athb_core.cu", "athb_dropin.cu", "athb_batch.cu", "athb_noalloc.cu", "athb_output.cu", "athb_adjoint.cu",
               "athb_problems_dev.cu"]
 CPP_SOURCES = ["athinput.cpp", "problems.cpp"]
-HEADERS = ["dual.cuh", "mhd_physics.cuh", "step_types.cuh", "step_kernels.cuh", "athb_internal.h"]
+HEADERS = ["dual.cuh", "mhd_physics.cuh", "step_types.cuh", "step_kernels.cuh", "athb_internal.h", "mhd_adjoint.cuh",
+           "step_generic.cuh", "step_adjoint.cuh", "adjoint_driver.cuh"]
 
 
 def _run(cmd: list[str], verbose: bool) -> str:

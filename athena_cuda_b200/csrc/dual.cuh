@@ -12,10 +12,13 @@
 // step takes ("frozen" branches); the adjoint kernels (mhd_adjoint.cuh) make
 // the same choices, which is what makes them exact transposes of each other.
 //
-// Non-differentiable points: sqrt(0) is given a zero derivative when its
-// argument's tangent is exactly zero (the field-free regions of a problem keep
-// B = 0 under any perturbation that leaves B alone), fabs(0) differentiates as
-// +x, and MAX/MIN pick the operand the value comparison picks.
+// Non-differentiable points: sqrt(0) is given a zero derivative.  Exact zeros
+// under a square root come from field-free regions (|B| = 0, where the
+// eigenvector formulas switch branch) and from squares of the tiny fields that
+// numerical diffusion leaks into them (|B| ~ 1e-160 squares to 0.0); in both
+// the derivative of the square root is unbounded while that of the function it
+// belongs to (|B|, the Alfven speed) is not.  fabs(0) differentiates as +x,
+// and MAX/MIN pick the operand the value comparison picks.
 #pragma once
 
 #include <math.h>
@@ -77,9 +80,12 @@ using ::fabs;
 using ::sqrt;
 ATHB_DHD Dual sqrt(Dual a) {
   const double s = ::sqrt(a.v);
-  return Dual(s, a.t == 0.0 ? 0.0 : a.t / (2.0 * s));
+  return Dual(s, s > 0.0 ? a.t / (2.0 * s) : 0.0);
 }
 ATHB_DHD Dual fabs(Dual a) { return a.v < 0.0 ? -a : a; }
+
+// the same value with no derivative
+ATHB_DHD Dual no_tangent(Dual a) { return Dual(a.v, 0.0); }
 
 // value of a scalar of either kind
 ATHB_DHD double value_of(double a) { return a; }

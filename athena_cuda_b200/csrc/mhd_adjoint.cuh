@@ -186,7 +186,7 @@ ATHB_HD void esys_prim_adj(double d, double v1, double p, double b1, double b2, 
     cfsqb += Asb / cf2_cs2; asqb -= Asb / cf2_cs2; c2b -= Asb * As / cf2_cs2;
   }
   double btsqb = 0.0;
-  if (bt != 0.0) {
+  if (bt != 0.0 && !(btsq < kBetaFreeze * (b1 * b1 + d * asq))) {   // freeze_beta
     const double btb = -bet2b * bet2 / bt - bet3b * bet3 / bt;
     b2b += bet2b / bt;
     b3b += bet3b / bt;
@@ -260,6 +260,7 @@ ATHB_HD void prim_right_col_adj(int n, const double rb[7], PrimEig& Eb) {
 }
 
 ATHB_HD void zero(PrimEig& E) {
+  #pragma unroll
   for (int n = 0; n < 7; n++) E.ev[n] = 0.0;
   E.R00 = E.R02 = E.R10 = E.R12 = E.R20 = E.R21 = E.R22 = E.R30 = E.R31 = E.R32 = 0.0;
   E.R40 = E.R42 = E.R50 = E.R51 = E.R52 = E.R60 = E.R61 = E.R62 = 0.0;
@@ -286,6 +287,7 @@ ATHB_HD void plm_cell_adj(const Prim1& wm, const Prim1& w0, const Prim1& wp, dou
   double Wm[7], W0[7], Wp[7];
   prim_arr(wm, Wm); prim_arr(w0, W0); prim_arr(wp, Wp);
   double dWc[7], dWl[7], dWr[7], dWg[7];
+  #pragma unroll
   for (int n = 0; n < 7; n++) {
     dWc[n] = Wp[n] - Wm[n];
     dWl[n] = W0[n] - Wm[n];
@@ -299,6 +301,7 @@ ATHB_HD void plm_cell_adj(const Prim1& wm, const Prim1& w0, const Prim1& wp, dou
   prim_project(E, dWr, dar);
   prim_project(E, dWg, dag);
   double da[7];
+  #pragma unroll
   for (int n = 0; n < 7; n++) {
     da[n] = 0.0;
     if (dal[n] * dar[n] > 0.0) {
@@ -315,8 +318,9 @@ ATHB_HD void plm_cell_adj(const Prim1& wm, const Prim1& w0, const Prim1& wp, dou
   dWm[4] = da[0] * E.R40 + da[2] * E.R42 + da[4] * E.R42 + da[6] * E.R40;
   dWm[5] = da[0] * E.R50 + da[1] * E.R51 + da[2] * E.R52 + da[4] * E.R52 + da[5] * E.R51 + da[6] * E.R50;
   dWm[6] = da[0] * E.R60 + da[1] * E.R61 + da[2] * E.R62 + da[4] * E.R62 + da[5] * E.R61 + da[6] * E.R60;
-  double l0v[7], r0v[7], dW[7];
+  double dW[7];
   unsigned lsel = 0, rsel = 0;  // 2 bits per component: 0 = own value, 1 = first clip operand, 2 = second
+  #pragma unroll
   for (int n = 0; n < 7; n++) {
     const double l0 = W0[n] - 0.5 * dWm[n];
     const double r0 = W0[n] + 0.5 * dWm[n];
@@ -333,8 +337,6 @@ ATHB_HD void plm_cell_adj(const Prim1& wm, const Prim1& w0, const Prim1& wp, dou
     if (hir < r) { r = hir; sr = 2; }
     lsel |= sl << (2 * n);
     rsel |= sr << (2 * n);
-    l0v[n] = l;
-    r0v[n] = r;
     dW[n] = r - l;
   }
   const double qx = 0.5 * rmax(E.ev[6], 0.0) * dtodx;
@@ -348,22 +350,27 @@ ATHB_HD void plm_cell_adj(const Prim1& wm, const Prim1& w0, const Prim1& wp, dou
   zero(Eb);
   double dWb[7] = {0, 0, 0, 0, 0, 0, 0};
   // step 9, second loop (waves moving left)
+  #pragma unroll
   for (int n = 6; n >= 0; n--) {
     if (!(E.ev[n] < 0.)) continue;
     double l[7], r[7], h[7], lb[7] = {0, 0, 0, 0, 0, 0, 0}, rb[7] = {0, 0, 0, 0, 0, 0, 0};
     prim_left_row(E, n, l);
     prim_right_col(E, n, r);
+    #pragma unroll
     for (int m = 0; m < 7; m++) h[m] = l[m] * 0.5 * dtodx;
     double hb[7] = {0, 0, 0, 0, 0, 0, 0};
     const int lm = prim_left_mask(n), rm = prim_right_mask(n);
     {  // pWl[m] -= qa2 * r[m], qa2 = sum h[m] dev2 dW[m], dev2 = ev[n] - ev[6]
       const double dev2 = E.ev[n] - E.ev[6];
       double qa2 = 0.0, hdw = 0.0;
+      #pragma unroll
       for (int m = 0; m < 7; m++)
         if ((lm >> m) & 1) { qa2 += h[m] * dev2 * dW[m]; hdw += h[m] * dW[m]; }
       double qa2b = 0.0;
+      #pragma unroll
       for (int m = 0; m < 7; m++)
         if ((rm >> m) & 1) { qa2b -= pWlb[m] * r[m]; rb[m] -= qa2 * pWlb[m]; }
+      #pragma unroll
       for (int m = 0; m < 7; m++)
         if ((lm >> m) & 1) { hb[m] += qa2b * dev2 * dW[m]; dWb[m] += qa2b * h[m] * dev2; }
       const double dev2b = qa2b * hdw;
@@ -373,17 +380,21 @@ ATHB_HD void plm_cell_adj(const Prim1& wm, const Prim1& w0, const Prim1& wp, dou
     if (n != 0) {  // pWr[m] += qa * r[m], qa = sum h[m] dev dW[m], dev = ev[0] - ev[n]
       const double dev = E.ev[0] - E.ev[n];
       double qa = 0.0, hdw = 0.0;
+      #pragma unroll
       for (int m = 0; m < 7; m++)
         if ((lm >> m) & 1) { qa += h[m] * dev * dW[m]; hdw += h[m] * dW[m]; }
       double qab = 0.0;
+      #pragma unroll
       for (int m = 0; m < 7; m++)
         if ((rm >> m) & 1) { qab += pWrb[m] * r[m]; rb[m] += qa * pWrb[m]; }
+      #pragma unroll
       for (int m = 0; m < 7; m++)
         if ((lm >> m) & 1) { hb[m] += qab * dev * dW[m]; dWb[m] += qab * h[m] * dev; }
       const double devb = qab * hdw;
       Eb.ev[0] += devb;
       Eb.ev[n] -= devb;
     }
+    #pragma unroll
     for (int m = 0; m < 7; m++) {
       lb[m] += hb[m] * 0.5 * dtodx;
       dtodxb += hb[m] * l[m] * 0.5;
@@ -392,6 +403,7 @@ ATHB_HD void plm_cell_adj(const Prim1& wm, const Prim1& w0, const Prim1& wp, dou
     prim_right_col_adj(n, rb, Eb);
   }
   // step 9, first loop (waves moving right)
+  #pragma unroll
   for (int n = 5; n >= 0; n--) {
     if (!(E.ev[n] > 0.)) continue;
     double l[7], r[7], lb[7] = {0, 0, 0, 0, 0, 0, 0}, rb[7] = {0, 0, 0, 0, 0, 0, 0};
@@ -400,11 +412,14 @@ ATHB_HD void plm_cell_adj(const Prim1& wm, const Prim1& w0, const Prim1& wp, dou
     const int lm = prim_left_mask(n), rm = prim_right_mask(n);
     const double dev = E.ev[6] - E.ev[n];
     double qa = 0.0, ldw = 0.0;
+    #pragma unroll
     for (int m = 0; m < 7; m++)
       if ((lm >> m) & 1) { qa += l[m] * 0.5 * dtodx * dev * dW[m]; ldw += l[m] * dW[m]; }
     double qab = 0.0;
+    #pragma unroll
     for (int m = 0; m < 7; m++)
       if ((rm >> m) & 1) { qab += pWlb[m] * r[m]; rb[m] += qa * pWlb[m]; }
+    #pragma unroll
     for (int m = 0; m < 7; m++)
       if ((lm >> m) & 1) {
         lb[m] += qab * 0.5 * dtodx * dev * dW[m];
@@ -420,6 +435,7 @@ ATHB_HD void plm_cell_adj(const Prim1& wm, const Prim1& w0, const Prim1& wp, dou
   // step 8: pWl = Wrv - qx dW, pWr = Wlv + qy dW
   double Wlvb[7], Wrvb[7];
   double qxb = 0.0, qyb = 0.0;
+  #pragma unroll
   for (int n = 0; n < 7; n++) {
     Wrvb[n] = pWlb[n];
     qxb -= pWlb[n] * dW[n];
@@ -435,6 +451,7 @@ ATHB_HD void plm_cell_adj(const Prim1& wm, const Prim1& w0, const Prim1& wp, dou
   // step 7: dW = r - l, and the clips
   double Wmb[7] = {0, 0, 0, 0, 0, 0, 0}, W0b[7] = {0, 0, 0, 0, 0, 0, 0}, Wpb[7] = {0, 0, 0, 0, 0, 0, 0};
   double dWmb[7];
+  #pragma unroll
   for (int n = 0; n < 7; n++) {
     Wrvb[n] += dWb[n];
     Wlvb[n] -= dWb[n];
@@ -472,6 +489,7 @@ ATHB_HD void plm_cell_adj(const Prim1& wm, const Prim1& w0, const Prim1& wp, dou
   // step 4: limiter, branch frozen
   double dacb[7] = {0, 0, 0, 0, 0, 0, 0}, dalb[7] = {0, 0, 0, 0, 0, 0, 0};
   double darb[7] = {0, 0, 0, 0, 0, 0, 0}, dagb[7] = {0, 0, 0, 0, 0, 0, 0};
+  #pragma unroll
   for (int n = 0; n < 7; n++) {
     if (!(dal[n] * dar[n] > 0.0)) continue;
     const double sg = rsign(dac[n]);
@@ -495,6 +513,7 @@ ATHB_HD void plm_cell_adj(const Prim1& wm, const Prim1& w0, const Prim1& wp, dou
   prim_project_adj(E, dWr, darb, dWrb, Eb);
   prim_project_adj(E, dWg, dagb, dWgb, Eb);
   // step 2: differences and the van Leer mean
+  #pragma unroll
   for (int n = 0; n < 7; n++) {
     if (dWl[n] * dWr[n] > 0.0) {
       const double s = dWl[n] + dWr[n];
@@ -729,7 +748,7 @@ ATHB_HD void roe_scalars_adj(const RoeAvg& r, const RoeSpeeds& s, double b1, con
   const double sgb = -bet2sb * bet2s / sg - bet3sb * bet3s / sg;
   sb.gfac += sqrt_adj(sg, sgb);
   double b2b = Sb.b2, b3b = Sb.b3;
-  if (bt != 0.0) {
+  if (bt != 0.0 && !(s.btsq < kBetaFreeze * (b1 * b1 + d * s.twid_asq))) {   // freeze_beta
     const double btb = -bet2b * bet2 / bt - bet3b * bet3 / bt;
     b2b += bet2b / bt;
     b3b += bet3b / bt;
@@ -978,6 +997,7 @@ ATHB_HD void flux_hlle_adj(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, co
   Cons1 Flb, Frb;
   double* flb = &Flb.d;
   double* frb = &Frb.d;
+  #pragma unroll
   for (int k = 0; k < 7; k++) {
     flb[k] = (0.5 + t) * fb[k];
     frb[k] = (0.5 - t) * fb[k];
@@ -1105,9 +1125,11 @@ ATHB_HD void flux_roe_adj(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, con
   // the forward's intermediate-state test (the HLLE fallback, frozen)
   {
     double u[7] = {Ul.d, Ul.mx, Ul.my, Ul.mz, Ul.e, Ul.by, Ul.bz};
+    #pragma unroll
     for (int n = 0; n < 6; n++) {
       double c[7];
       roe_right_col(S, ev, n, c);
+      #pragma unroll
       for (int m = 0; m < 7; m++)
         if ((roe_right_mask(n) >> m) & 1) u[m] += a[n] * c[m];
       if (ev[n + 1] > ev[n]) {
@@ -1129,17 +1151,20 @@ ATHB_HD void flux_roe_adj(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, con
   RoeScal Sb;
   zero(Sb);
   double evb[7] = {0, 0, 0, 0, 0, 0, 0}, abar[7];
+  #pragma unroll
   for (int n = 0; n < 7; n++) {
     double c[7], cb[7];
     roe_right_col(S, ev, n, c);
     const double coeff = 0.5 * rmax(fabs(ev[n]), 0.0) * a[n];
     double coeffb = 0.0;
+    #pragma unroll
     for (int k = 0; k < 7; k++) {
       if ((roe_right_mask(n) >> k) & 1) { coeffb -= fb[k] * c[k]; cb[k] = -coeff * fb[k]; }
       else cb[k] = 0.0;
     }
     abar[n] = 0.5 * fabs(ev[n]) * coeffb;
-    evb[n] += 0.5 * fabs_d(ev[n]) * a[n] * coeffb;
+    // MAX(fabs(ev), 0) takes the constant 0 when ev == 0
+    if (fabs(ev[n]) > 0.0) evb[n] += 0.5 * fabs_d(ev[n]) * a[n] * coeffb;
     roe_right_col_adj(S, ev, n, cb, Sb, evb);
   }
   double dUb[7] = {0, 0, 0, 0, 0, 0, 0};
@@ -1214,10 +1239,11 @@ ATHB_HD void cell_dti_adj(double d, double m1, double m2, double m3, double e, c
   const double asq = eos.gamma * p * di;
   const double ca = sqrt(asq);
   const double t1 = (fabs(v1) + ca) / dx1, t2 = (fabs(v2) + ca) / dx2;
-  double m = rmax(0.0, t1);
+  // m = MAX(MAX(0, t1), t2): MAX(a, b) = (a > b) ? a : b takes b on a tie
+  const double m = rmax(0.0, t1);
   double v1b = 0.0, v2b = 0.0, cab = 0.0;
-  if (t2 > m) { v2b += fabs_d(v2) * mb / dx2; cab += mb / dx2; }
-  else if (0.0 < t1) { v1b += fabs_d(v1) * mb / dx1; cab += mb / dx1; }
+  if (!(m > t2)) { v2b += fabs_d(v2) * mb / dx2; cab += mb / dx2; }
+  else if (!(0.0 > t1)) { v1b += fabs_d(v1) * mb / dx1; cab += mb / dx1; }
   const double asqb = sqrt_adj(ca, cab);
   const double pb = asqb * eos.gamma * di;
   double dib = asqb * eos.gamma * p;

@@ -30,6 +30,8 @@
 
 #include <math.h>
 
+#include <type_traits>
+
 #include "dual.cuh"
 
 #if defined(__CUDACC__)
@@ -41,6 +43,24 @@
 namespace athb {
 
 constexpr double kTiny = 1.0e-20;   // TINY_NUMBER, src/defs.h:100
+
+// Derivatives only (the tangent-linear model and the adjoint; the plain step
+// is untouched): the unit vector of the transverse field, (b2, b3)/|b_t|,
+// turns at a rate ~1/|b_t|, and near |b_t| = 0 the wave terms that carry it
+// cancel in exact arithmetic but not in floating point, whereas their exact
+// contribution to the derivative is O(|b_t|).  Where the transverse magnetic
+// pressure is below kBetaFreeze times the pressure scale (b_n^2 + d a^2) the
+// unit vector is therefore differentiated as a constant.
+constexpr double kBetaFreeze = 1.0e-12;
+template <class T>
+ATHB_HD void freeze_beta(T& bet2, T& bet3, double btsq, double scale) {
+  if constexpr (!std::is_same<T, double>::value) {
+    if (btsq < kBetaFreeze * scale) {
+      bet2 = no_tangent(bet2);
+      bet3 = no_tangent(bet3);
+    }
+  }
+}
 
 // Conserved / primitive variables of one 1D slice, in the slice frame
 // (x = sweep direction).  Field order is that of Cons1D / Prim1D
@@ -139,6 +159,7 @@ ATHB_HD void esys_prim(T d, T v1, T p, T b1, T b2, T b3,
   const T bt = sqrt(btsq);
   T bet2, bet3;
   if (bt == 0.0) { bet2 = 1.0; bet3 = 0.0; } else { bet2 = b2 / bt; bet3 = b3 / bt; }
+  freeze_beta(bet2, bet3, value_of(btsq), value_of(b1) * value_of(b1) + value_of(d) * value_of(asq));
 
   T alpha_f, alpha_s;
   if (cf2_cs2 == 0.0) { alpha_f = 1.0; alpha_s = 0.0; }
@@ -482,6 +503,7 @@ ATHB_HD void roe_scalars(const RoeAvgT<T>& r, const RoeSpeedsT<T>& s, T b1, cons
   const T bt_star = sqrt(s.bt_starsq);
   T bet2, bet3;
   if (bt == 0.0) { bet2 = 1.0; bet3 = 0.0; } else { bet2 = b2 / bt; bet3 = b3 / bt; }
+  freeze_beta(bet2, bet3, value_of(s.btsq), value_of(b1) * value_of(b1) + value_of(d) * value_of(s.twid_asq));
   const T sg = sqrt(s.gfac);
   const T bet2_star = bet2 / sg;
   const T bet3_star = bet3 / sg;

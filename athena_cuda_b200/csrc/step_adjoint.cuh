@@ -68,12 +68,12 @@ struct AdjArgs {
   double dx1, dx2;
   Eos eos;
   ATHB_MEM long long o(int j, int i) const { return (long long)j * pitch + i; }
-  ATHB_MEM double s(int p, long long off) const { return in[p * ps + off]; }
-  ATHB_MEM double t(int p, long long off) const { return tape[p * ps + off]; }
-  ATHB_MEM double lo(int p, long long off) const { return lout[p * ps + off]; }
-  ATHB_MEM double& li(int p, long long off) const { return lin[p * ps + off]; }
-  ATHB_MEM double& a(int p, long long off) const { return adj[p * ps + off]; }
-  ATHB_MEM double av(int p, long long off) const { return adj[p * ps + off]; }
+  ATHB_MEM double s(int p, long long off) const { ATHB_CHECK_OFF(off, ps); return in[p * ps + off]; }
+  ATHB_MEM double t(int p, long long off) const { ATHB_CHECK_OFF(off, ps); return tape[p * ps + off]; }
+  ATHB_MEM double lo(int p, long long off) const { ATHB_CHECK_OFF(off, ps); return lout[p * ps + off]; }
+  ATHB_MEM double& li(int p, long long off) const { ATHB_CHECK_OFF(off, ps); return lin[p * ps + off]; }
+  ATHB_MEM double& a(int p, long long off) const { ATHB_CHECK_OFF(off, ps); return adj[p * ps + off]; }
+  ATHB_MEM double av(int p, long long off) const { ATHB_CHECK_OFF(off, ps); return adj[p * ps + off]; }
 };
 
 ATHB_HD bool in_range(const GenRange& r, int j, int i) { return j >= r.j0 && j <= r.j1 && i >= r.i0 && i <= r.i1; }
@@ -154,7 +154,6 @@ ATHB_HD void adj_update(const AdjArgs& a, int j, int i) {
     double lb = a.lo(P_B1I, o);
     if (i <= a.ie) lb += 0.5 * a.lo(P_B1C, o);
     if (i - 1 >= a.is) lb += 0.5 * a.lo(P_B1C, o - 1);
-    if (i == a.ie + 1) lb = a.lo(P_B1I, o) + 0.5 * a.lo(P_B1C, o - 1);
     a.a(A_LB1, o) = lb;
     a.li(P_B1I, o) += lb;
     dtb += -lb * (a.t(G_EMF1, o + P) - a.t(G_EMF1, o)) / a.dx2;
@@ -529,7 +528,7 @@ ATHB_HD void adj_emf0(const AdjArgs& a, int j, int i) {
 // (transverse terms), correct_e and the half-step corner emf; items over
 // [is-2, ie+2] x [js-2, je+2].
 ATHB_HD void adj_flux1(const AdjArgs& a, int j, int i) {
-  const long long o = a.o(j, i), P = a.pitch;
+  const long long o = a.o(j, i);
   const StepCoef<double>& c = a.c;
   const GenRange CX = range_correct_x(a.is, a.ie, a.js, a.je), CY = range_correct_y(a.is, a.ie, a.js, a.je);
   const GenRange E = range_correct_e(a.is, a.ie, a.js, a.je), K = range_emf0(a.is, a.ie, a.js, a.je);
@@ -640,7 +639,7 @@ ATHB_HD void adj_sources(const AdjArgs& a, int j, int i) {
   };
   // cell (j,i)
   if (in_range(range_correct_e(a.is, a.ie, a.js, a.je), j, i)) {
-    const double B1 = a.s(P_B1C, o), B2 = a.s(P_B2C, o), B3 = a.s(P_B3C, o);
+    const double B3 = a.s(P_B3C, o);
     const double d = a.s(P_D, o), V3 = a.s(P_M3, o) / d;
     double lB1 = 0, lB2 = 0, lB3 = 0, lV3 = 0;
     if (in_range(CX, j, i + 1)) {  // ul of x face (j,i+1)
@@ -796,6 +795,8 @@ ATHB_HD void adj_prim_gather(const AdjArgs& a, int dir, int j, int i) {
 // ===========================================================================
 // Ghost zones (src/set_bvals.c:114-145): the generic fill and its adjoint.
 // ===========================================================================
+constexpr int kNghostA = 4;   // ghost layers (nghost, src/defs.h:82)
+
 struct GhostGeom {
   int is, ie, js, je, sx, sy;
   int bc[4];
@@ -855,8 +856,9 @@ ATHB_HD void fold_x2(double* l, long long ps, int pitch, const GhostGeom& g, int
     const int je_int = g.je + (kind == 2 ? 1 : 0);
     if (j < g.js || j > je_int) continue;
     const long long o = (long long)j * pitch + i;
-    for (int jj = 0; jj < g.sy; jj++) {
-      if (jj >= g.js && jj <= je_int) continue;
+    for (int gq = 0; gq < 2 * kNghostA; gq++) {   // the ghost rows: js-4..js-1, je_int+1..je_int+4
+      const int jj = gq < kNghostA ? g.js - kNghostA + gq : je_int + 1 + (gq - kNghostA);
+      if (jj < 0 || jj >= g.sy) continue;
       bool f = false;
       if (ghost_map1(jj, g.js, g.je, kind == 2, g.bc[2], g.bc[3], f) != j) continue;
       const long long q = (long long)jj * pitch + i;
@@ -877,8 +879,9 @@ ATHB_HD void fold_x1(double* l, long long ps, int pitch, const GhostGeom& g, int
     const int ie_int = g.ie + (kind == 1 ? 1 : 0), je_int = g.je + (kind == 2 ? 1 : 0);
     if (j < g.js || j > je_int || i < g.is || i > ie_int) continue;
     const long long o = (long long)j * pitch + i;
-    for (int ii = 0; ii < g.sx; ii++) {
-      if (ii >= g.is && ii <= ie_int) continue;
+    for (int gq = 0; gq < 2 * kNghostA; gq++) {   // the ghost columns: is-4..is-1, ie_int+1..ie_int+4
+      const int ii = gq < kNghostA ? g.is - kNghostA + gq : ie_int + 1 + (gq - kNghostA);
+      if (ii < 0 || ii >= g.sx) continue;
       bool f = false;
       if (ghost_map1(ii, g.is, g.ie, kind == 1, g.bc[0], g.bc[1], f) != i) continue;
       const long long q = (long long)j * pitch + ii;

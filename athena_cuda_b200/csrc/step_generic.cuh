@@ -49,20 +49,22 @@ template <> struct Planes<Dual> {
 };
 
 // Tape / scratch planes of the generic step (each group of 7 is one Cons1 or
-// Prim1 in the sweep frame).
+// Prim1 in the sweep frame), laid out as the fast kernels' scratch planes
+// (step_types.cuh) followed by the taped planes, so that a taped step of the
+// fast kernels and one of the generic step leave the same tape.
 enum GenPlane {
-  G_WLNX = 0,    // W_L at face i+1/2 from cell i (x sweep), after the source term
-  G_WRTX = 7,    // W_R at face i-1/2 from cell i
-  G_WLNY = 14,
-  G_WRTY = 21,
-  G_ULX = 28, G_URX = 35, G_FX = 42,   // predictor states and fluxes at x faces
-  G_ULY = 49, G_URY = 56, G_FY = 63,
-  G_FX2 = 70, G_FY2 = 77,              // corrector fluxes
-  G_ECC0 = 84,   // cell emf3 at t^n
-  G_EMF0 = 85,   // corner emf at t^n (half step)
-  G_ECC1 = 86,   // cell emf3 at t^{n+1/2}
-  G_EMF1 = 87,   // corner emf for the full step
-  NGEN = 88
+  G_ULX = S_ULX, G_URX = S_URX, G_FX = S_FX,   // predictor states and fluxes at x faces
+  G_ULY = S_ULY, G_URY = S_URY, G_FY = S_FY,
+  G_FX2 = S_FX2, G_FY2 = S_FY2,                // corrector fluxes
+  G_ECC1 = S_ECC,   // cell emf3 at t^{n+1/2}
+  G_EMF1 = S_EMF,   // corner emf of the full step
+  G_WLNX = T_WLNX,  // W_L at face i+1/2 from cell i (x sweep), after the source term
+  G_WRTX = T_WRTX,  // W_R at face i-1/2 from cell i
+  G_WLNY = T_WLNY,
+  G_WRTY = T_WRTY,
+  G_ECC0 = T_ECC0,  // cell emf3 at t^n
+  G_EMF0 = T_EMF0,  // corner emf at t^n (half step)
+  NGEN = NTAPED
 };
 
 // dt and its derived factors (src/__integrate_2d__.c:102-110), as the scalar
@@ -83,6 +85,23 @@ ATHB_HD StepCoef<T> make_coef(T dt, double dx1, double dx2) {
   return c;
 }
 
+// Host test builds define ATHB_HOST_BOUNDS: every plane access is checked to
+// stay inside its plane (the kernels' index ranges are verified on the CPU).
+#if defined(ATHB_HOST_BOUNDS) && !defined(__CUDA_ARCH__)
+#include <cstdio>
+#include <cstdlib>
+#define ATHB_CHECK_OFF(off, ps)                                                           \
+  do {                                                                                    \
+    if ((off) < 0 || (off) >= (ps)) {                                                     \
+      std::fprintf(stderr, "plane offset %lld outside [0, %lld) at %s:%d\n", (long long)(off), \
+                   (long long)(ps), __FILE__, __LINE__);                                  \
+      std::abort();                                                                       \
+    }                                                                                     \
+  } while (0)
+#else
+#define ATHB_CHECK_OFF(off, ps) do { } while (0)
+#endif
+
 template <class T> struct GenArgs {
   Planes<T> in, out, scr;
   const StepCoef<T>* coef;
@@ -92,9 +111,9 @@ template <class T> struct GenArgs {
   double dx1, dx2;
   Eos eos;
   ATHB_MEM long long o(int j, int i) const { return (long long)j * pitch + i; }
-  ATHB_MEM T s(int p, long long off) const { return in.get(p * ps + off); }
-  ATHB_MEM T g(int p, long long off) const { return scr.get(p * ps + off); }
-  ATHB_MEM void put(int p, long long off, T x) const { scr.set(p * ps + off, x); }
+  ATHB_MEM T s(int p, long long off) const { ATHB_CHECK_OFF(off, ps); return in.get(p * ps + off); }
+  ATHB_MEM T g(int p, long long off) const { ATHB_CHECK_OFF(off, ps); return scr.get(p * ps + off); }
+  ATHB_MEM void put(int p, long long off, T x) const { ATHB_CHECK_OFF(off, ps); scr.set(p * ps + off, x); }
 };
 
 // Ranges (inclusive) of the stages over an interior [is,ie] x [js,je].

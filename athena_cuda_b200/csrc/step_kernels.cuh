@@ -113,7 +113,14 @@ inline PredictGeom make_predict_geom(int nx1, int nx2, int ly) {
 // ---------------------------------------------------------------------------
 // k_predict: predictor L/R states and fluxes of both sweeps.
 // ---------------------------------------------------------------------------
-template <int FLUX>
+// TAPE: also keep the face states W_L, W_R of every predictor face in the
+// T_WLN* / T_WRT* planes (the recorded step of the adjoint).
+__device__ __forceinline__ void store_prim(double* base, long long ps, long long o, const Prim1& w) {
+  base[0 * ps + o] = w.d; base[1 * ps + o] = w.vx; base[2 * ps + o] = w.vy; base[3 * ps + o] = w.vz;
+  base[4 * ps + o] = w.p; base[5 * ps + o] = w.by; base[6 * ps + o] = w.bz;
+}
+
+template <int FLUX, bool TAPE = false>
 __device__ __forceinline__ void predict_x(const GridArgs& g, int bx, int by) {
   const StepState& st = *g.st;
   const int lane = threadIdx.x & 31;
@@ -148,6 +155,10 @@ __device__ __forceinline__ void predict_x(const GridArgs& g, int bx, int by) {
     store_cons(g.scr + S_ULX * g.ps, g.ps, o, ul);
     store_cons(g.scr + S_URX * g.ps, g.ps, o, ur);
     store_cons(g.scr + S_FX * g.ps, g.ps, o, riemann<FLUX>(ul, ur, wl, wrt, b1l, g.eos));
+    if constexpr (TAPE) {
+      store_prim(g.scr + T_WLNX * g.ps, g.ps, o - 1, wl);
+      store_prim(g.scr + T_WRTX * g.ps, g.ps, o, wrt);
+    }
   }
   // step 3: emf3_cc at t^n on [is-2,ie+2] x [js-2,je+2] (src/__integrate_2d__.c:249-255)
   if ((lane >= 1 || bx == 0) && c <= g.ie + 2) {
@@ -171,7 +182,7 @@ __device__ __forceinline__ Prim1 sh_load(const double* sh, int slot, int tid) {
   return w;
 }
 
-template <int FLUX>
+template <int FLUX, bool TAPE = false>
 __device__ __forceinline__ void predict_y(const GridArgs& g, const PredictGeom& pg, int b) {
   // slots 0..2: prims of rows k-1, k, k+1 (ring); slot 3: W_L of face k
   __shared__ double sh[4 * 7 * kThreads];
@@ -207,6 +218,10 @@ __device__ __forceinline__ void predict_y(const GridArgs& g, const PredictGeom& 
       store_cons(g.scr + S_ULY * g.ps, g.ps, o, ul);
       store_cons(g.scr + S_URY * g.ps, g.ps, o, ur);
       store_cons(g.scr + S_FY * g.ps, g.ps, o, riemann<FLUX>(ul, ur, wl, wrt, b2l, g.eos));
+      if constexpr (TAPE) {
+        store_prim(g.scr + T_WLNY * g.ps, g.ps, o - g.pitch, wl);
+        store_prim(g.scr + T_WRTY * g.ps, g.ps, o, wrt);
+      }
     }
     sh_store(sh, 3, tid, wln);
     r0 = r1;
@@ -223,20 +238,20 @@ constexpr int kCorrectMinBlocks = 4;
 // come first and the short role-X row segments (31 faces) last, so the
 // block scheduler ends the launch on small blocks instead of a tail of
 // marches.
-template <int FLUX>
+template <int FLUX, bool TAPE = false>
 __device__ __forceinline__ void predict_block(const GridArgs& g, const PredictGeom& pg, int b) {
   if (b < pg.ny_blocks) {
-    predict_y<FLUX>(g, pg, b);
+    predict_y<FLUX, TAPE>(g, pg, b);
   } else {
     b -= pg.ny_blocks;
-    predict_x<FLUX>(g, b % pg.xseg, b / pg.xseg);
+    predict_x<FLUX, TAPE>(g, b % pg.xseg, b / pg.xseg);
   }
 }
 
-template <int FLUX>
+template <int FLUX, bool TAPE = false>
 static __global__ void __launch_bounds__(kThreads, kPredictMinBlocks) k_predict(GridArgs g, PredictGeom pg) {
   if (g.st->done) return;
-  predict_block<FLUX>(g, pg, blockIdx.x);
+  predict_block<FLUX, TAPE>(g, pg, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------

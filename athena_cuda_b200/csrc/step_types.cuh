@@ -19,6 +19,18 @@ enum ScratchPlane {
   NSCRATCH = 58
 };
 
+// Planes after the scratch planes that a recorded ("taped") step keeps for
+// the adjoint: the predictor's face states in primitive form (W_L of the
+// face on the right of a cell, W_R of the face on its left; each group of 7
+// is one Prim1 in the sweep frame) and the half-step emfs, which the plain
+// step overwrites.
+enum TapePlane {
+  T_WLNX = NSCRATCH, T_WRTX = NSCRATCH + 7, T_WLNY = NSCRATCH + 14, T_WRTY = NSCRATCH + 21,
+  T_ECC0 = NSCRATCH + 28,   // cell emf3 at t^n
+  T_EMF0 = NSCRATCH + 29,   // corner emf of the half step
+  NTAPED = NSCRATCH + 30
+};
+
 enum BcKind { BC_REFLECT = 1, BC_OUTFLOW = 2, BC_PERIODIC = 4 };
 
 // Device-resident time-stepping state of one grid.

@@ -72,7 +72,11 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="field_loop", choices=["field_loop", "ensemble", "cpaw", "configs"])
+    ap.add_argument("--workload", default="field_loop", choices=["field_loop", "ensemble", "cpaw", "configs", "adjoint"])
+    ap.add_argument("--adj-cases", default="256x200,1024x2000",
+                    help="adjoint workload: comma-separated <N>x<steps> field-loop cases")
+    ap.add_argument("--adj-snapshot-gb", type=float, default=0.0,
+                    help="adjoint workload: device memory for checkpoints (0: most of the free memory)")
     ap.add_argument("--ensemble-n", type=int, default=512)
     ap.add_argument("--seq-sample", type=int, default=0,
                     help="time sequential single-grid runs on every k-th instance only (0: all)")
@@ -663,6 +667,59 @@ def configs_arm(a) -> None:
                       "cpu": cpu_model(), "rows": rows}))
 
 
+def adjoint_arm(a) -> None:
+    """Cost of the adjoint: the gradient of the field loop's final magnetic
+    energy with respect to its initial density (1 + 0.01 N(0,1) smoothed by a
+    4-cell Gaussian, seed 2024) over N x N cells and K steps, against a plain
+    forward solve of the same K steps (the graph-captured device loop).  Both
+    timed with a device synchronisation on each side (the adjoint call returns
+    synchronised); ratio = adjoint / forward, lower is better."""
+    import torch
+
+    from athena_cuda_b200 import Grid, Params, configs, problem_state, write_athinput
+    from athena_cuda_b200 import adjoint as fl
+
+    rows = []
+    with tempfile.TemporaryDirectory() as td:
+        for case in a.adj_cases.split(","):
+            n, k = (int(x) for x in case.split("x"))
+            blocks = configs.field_loop(n, n)
+            blocks["time"]["nlim"] = k
+            ath = write_athinput(Path(td) / f"athinput.{n}", blocks)
+            base = problem_state("field_loop", Params(ath))
+            S0 = fl.density_state(base, fl.smoothed_density(n, n, 2024))
+            g = Grid.from_athinput(ath, "field_loop")
+            # forward solve: loop entry (set_bvals, new_dt) then K steps
+            fwd = []
+            for _ in range(2):
+                g.upload(S0)
+                g.set_bvals()
+                g.new_dt()
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                g.run(k)
+                torch.cuda.synchronize()
+                fwd.append(time.perf_counter() - t0)
+            g.upload(S0)
+            snap = int(a.adj_snapshot_gb * 1e9)
+            t0 = time.perf_counter()
+            J, grad, st = g.adjoint_gradient(k, snapshot_bytes=snap)
+            t_adj = time.perf_counter() - t0
+            g.close()
+            grho = fl.density_gradient(base, grad)
+            t_fwd = min(fwd)
+            rows.append({"case": f"field loop {n}x{n}, {k} steps", "forward_s": t_fwd, "adjoint_s": t_adj,
+                         "ratio": t_adj / t_fwd, "J": J, "grad_rho_l2": float(np.sqrt(np.sum(grho * grho))),
+                         "adjoint_zone_cycles_per_s": n * n * k / t_adj, "stats": st})
+    head = rows[-1]
+    print(json.dumps({"metric": "adjoint/forward cost ratio (gradient of final magnetic energy w.r.t. initial "
+                                "density, field loop)", "value": head["ratio"], "unit": "x",
+                      "higher_is_better": False, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
+                      "config": {"workload": head["case"], "objective": "sum (B1c^2+B2c^2)/2",
+                                 "checkpointing": "binomial (revolve) state snapshots in HBM"},
+                      "rows": rows}))
+
+
 def measured_hbm_gbs():
     """HBM copy bandwidth measured on this GPU pool (MEASURED_PEAKS.json)."""
     f = ROOT / "MEASURED_PEAKS.json"
@@ -682,6 +739,8 @@ def main():
         cpaw_arm(a)
     elif a.workload == "configs":
         configs_arm(a)
+    elif a.workload == "adjoint":
+        adjoint_arm(a)
     else:
         ours(a)
 

@@ -295,6 +295,46 @@ int athb_batch_mode(const athb_batch *b);
  * is reported in *timed_out (1 expected) with the device still usable.      */
 int athb_batch_selftest_barrier(int device, long long spins, int *timed_out);
 
+/* ---- tangent-linear model and adjoint of the main loop --------------------- */
+/* No reference counterpart (the reference has no derivatives).  Both run the
+ * reference main loop (src/main.c:229-307: tlim clamp, integrate_2d,
+ * time += dt, new_dt, set_bvals) for nsteps iterations, or until tlim, from
+ * the context's resident state taken as the loop-entry state: set_bvals and
+ * new_dt (nstep 0 rule, src/new_dt.c:93-97) are applied to it first, so dt
+ * depends on the state as in the reference and is differentiated through
+ * the CFL max (the cell attaining it, lowest index on ties), the 2x growth cap
+ * and the tlim clamp.  Objective J = sum over interior cells of
+ * (B1c^2 + B2c^2)/2 at the final state.  Branches (limiters, upwinding,
+ * supersonic faces, the HLLE fallback of flux_roe) are those of the forward
+ * step.  The resident state and clock are left untouched.
+ * Host arrays use the athb_upload layout; only the cells a step writes are
+ * independent inputs (interior cells, B1i column ie+1, B2i row je+1): ghost
+ * entries of a direction are ignored and those of a gradient are zero.      */
+typedef struct athb_adjoint_stats {
+  int steps;                  /* iterations differentiated                    */
+  int snapshots;              /* state snapshots held in device memory        */
+  long long advances;         /* forward steps run (first sweep + recompute)  */
+  long long taped;            /* recorded forward steps (one per reverse step)*/
+  long long workspace_bytes;  /* device memory used, snapshots included       */
+  double seconds;             /* wall time of the call                        */
+  int tape_mode;              /* 1: every step's intermediates were kept by the
+                                 first sweep (no recorded re-step)            */
+} athb_adjoint_stats;
+/* Tangent-linear model: J and its directional derivative dJ along dstate0
+ * (host); dstate_out (host, may be NULL) receives the tangent of the final
+ * state, ghosts included.                                                   */
+int athb_tlm_run(athb_ctx *ctx, int nsteps, const double *dstate0, double *J, double *dJ, double *dstate_out);
+/* Adjoint: J and dJ/d(state) of the loop-entry state into grad (host, may be
+ * NULL).  Checkpointing: snapshot_bytes of device memory for snapshots
+ * (<= 0: 85% of the free memory less 1 GiB).  With room for every step's
+ * state and intermediates (the "tape", ~89 planes a step) the first sweep
+ * keeps them all and the reverse sweep recomputes nothing; with room for the
+ * states only the loop runs forward once and each reversed step is
+ * re-recorded from its state; with less, binomial checkpointing (Griewank
+ * 1992) recomputes the fewest forward steps the room allows.                */
+int athb_adjoint_gradient(athb_ctx *ctx, int nsteps, long long snapshot_bytes, double *J, double *grad,
+                          athb_adjoint_stats *stats);
+
 /* ---- allocation-free step ------------------------------------------------ */
 /* No counterpart in the reference.  One integrate_2d step (the cells
  * integrate_2d writes) from d_in into d_out, both caller-owned device buffers

@@ -123,7 +123,7 @@ static void eig_unflat(PrimEig& E, const double* b) {
 }
 
 static void check_esys(int trials) {
-  Stat st{"esys_prim"};
+  Stat st{"esys_prim"}, sd{"esys_prim_degen"};
   int cases[4] = {0, 0, 0, 0};
   for (int t = 0; t < trials; t++) {
     double x[6] = {U(0.2, 3), U(-1, 1), U(0.05, 2), U(-1.5, 1.5), U(-1.5, 1.5), U(-1.5, 1.5)};
@@ -142,7 +142,9 @@ static void check_esys(int trials) {
     double xb[6] = {0, 0, 0, 0, 0, 0};
     esys_prim_adj(x[0], x[1], x[2], x[3], x[4], x[5], EOS, Eb, xb[0], xb[1], xb[2], xb[3], xb[4], xb[5]);
     double rhs = 0; for (int k = 0; k < 6; k++) { rhs += xb[k] * xt[k]; sc = std::fmax(sc, std::fabs(xb[k] * xt[k])); }
-    st.add(lhs, rhs, sc);
+    // b2 = b3 = 0 with b1 != 0: alpha_s is the square root of a rounding
+    // residue, so both linearisations are ill-conditioned there
+    if (x[4] == 0.0 && x[5] == 0.0 && x[3] != 0.0) sd.add(lhs, rhs, sc); else st.add(lhs, rhs, sc);
     if (getenv("ESYS_DEBUG") && std::fabs(lhs - rhs) > 1e-10 * sc)
       printf("esys t=%d x=[%.6g %.6g %.6g %.6g %.6g %.6g] lhs=%.10g rhs=%.10g sc=%.3g\n", t, x[0], x[1], x[2], x[3], x[4], x[5], lhs, rhs, sc);
     cases[(x[4] == 0.0 ? 1 : 0) + (x[3] == 0.0 ? 2 : 0)]++;
@@ -150,6 +152,7 @@ static void check_esys(int trials) {
   char buf[128];
   snprintf(buf, sizeof buf, "(generic %d, bt=0 %d, b1=0 %d, both %d)", cases[0], cases[1], cases[2], cases[3]);
   st.print(buf);
+  sd.print("(b2 = b3 = 0, b1 != 0)");
 }
 
 static void check_plm(int trials) {
@@ -211,6 +214,9 @@ static int roe_path(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const Pri
 template <int FLUX>
 static void check_flux(int trials, const char* name) {
   Stat st{name};
+  char dname[64];
+  snprintf(dname, sizeof dname, "%s_degen", name);
+  Stat sd{dname};
   int paths[4] = {0, 0, 0, 0};
   for (int t = 0; t < trials; t++) {
     const int kind = t % 6;
@@ -240,7 +246,7 @@ static void check_flux(int trials, const char* name) {
     double rhs = bxb * bxt;
     for (int k = 0; k < 7; k++)
       rhs += (&ulb.d)[k] * tul[k] + (&urb.d)[k] * tur[k] + (&wlb.d)[k] * twl[k] + (&wrb.d)[k] * twr[k];
-    st.add(lhs, rhs, sc);
+    if (kind == 5 && bx != 0.0) sd.add(lhs, rhs, sc); else st.add(lhs, rhs, sc);
     if (getenv("FLUX_DEBUG") && std::fabs(lhs - rhs) > 1e-12 * sc)
       printf("%s t=%d kind=%d path=%d bx=%g rel=%.3e\n", name, t, kind, roe_path(ul, ur, wl, wr, bx),
              bx, std::fabs(lhs - rhs) / sc);
@@ -249,6 +255,7 @@ static void check_flux(int trials, const char* name) {
   snprintf(buf, sizeof buf, "(roe paths: subsonic %d, supersonic-left %d, supersonic-right %d, hlle-fallback %d)",
            paths[0], paths[1], paths[2], paths[3]);
   st.print(buf);
+  sd.print("(transverse field zero on both sides, normal field non-zero)");
 }
 
 static void check_emf(int trials) {

@@ -1,0 +1,208 @@
+"""The tangent-linear model and the adjoint on the GPU (athb_tlm_run,
+athb_adjoint_gradient through the C ABI).
+
+* the sm_100a kernels against the same code run on the host CPU
+  (tests/hostcheck): states and tangents bit for bit, gradients to the
+  rounding of the two reductions;
+* binomial checkpointing with a small snapshot budget gives the gradient of
+  storing every state, bit for bit;
+* the field-loop adjoint configuration (256 x 256, 200 steps; objective the
+  final magnetic energy, gradient with respect to the initial density
+  1 + 0.01 N(0,1) smoothed by a 4-cell Gaussian): the dot-product test
+  between the tangent-linear model and the adjoint, and central finite
+  differences (eps = 1e-6, 16 seeded directions) of the reference CPU path
+  (oracle/_ref, the reference's own sources) against the adjoint gradient;
+* the gradient wrapped in a torch.autograd.Function (test-side only).
+"""
+from __future__ import annotations
+
+import subprocess
+import tempfile
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import adjoint_host as ah
+import refutil
+from athena_cuda_b200 import Grid, Params, configs, problem_state, write_athinput
+from athena_cuda_b200 import adjoint as fl
+
+pytestmark = pytest.mark.gpu
+
+SMALL = {
+    "blast_mixed_bc": ("blast", configs.blast(20, 14, bc=(1, 2, 4, 2)), 8),
+    "field_loop": ("field_loop", configs.field_loop(24, 12), 8),
+    "random_noise_hlle": ("random", configs.field_loop(16, 12, flux="hlle"), 4),
+    "cpaw_tlim_clamp": ("cpaw2d", configs.cpaw2d(16, 8, tlim=0.05), 40),
+}
+
+
+def _small(name, tmp_path):
+    problem, blocks, n = SMALL[name]
+    p = Params.from_blocks(blocks)
+    cfg = p.config()
+    if problem == "random":
+        S0 = refutil.random_state(np.random.default_rng(5), cfg.nx1, cfg.nx2, False)
+    else:
+        S0 = problem_state(problem, p)
+    g = Grid.from_athinput(write_athinput(tmp_path / "athinput", blocks), "field_loop" if problem == "random" else problem)
+    g.upload(S0)
+    return cfg, S0, g, n
+
+
+@pytest.mark.parametrize("name", sorted(SMALL))
+def test_gpu_adjoint_and_tlm_match_host(name, tmp_path):
+    cfg, S0, g, n = _small(name, tmp_path)
+    J, grad, st = g.adjoint_gradient(n)
+    Jh, gh, steps, _ = ah.adjoint(cfg, S0, n, n + 1)
+    assert st["steps"] == steps
+    assert abs(J - Jh) <= 1e-13 * abs(Jh)
+    scale = np.max(np.abs(gh))
+    assert np.max(np.abs(grad - gh)) <= 1e-10 * scale, np.max(np.abs(grad - gh)) / scale
+    d = ah.interior_direction(np.random.default_rng(2), cfg)
+    Jt, dJ, dS = g.tlm(steps, d, want_state=True)
+    Jt_h, dJ_h, _, dS_h = ah.tlm(cfg, S0, d, steps)
+    assert np.array_equal(dS, dS_h)           # per-cell tangents: the same operations
+    assert abs(dJ - dJ_h) <= 1e-12 * abs(dJ_h)
+    ip = float(np.sum(grad * d))
+    assert abs(ip - dJ) <= 1e-11 * float(np.sum(np.abs(grad * d)))
+    # the resident state is untouched
+    assert np.array_equal(g.download()[0][:, 4:-4, 4:-4], S0[:, 4:-4, 4:-4])
+    g.close()
+
+
+def test_binomial_checkpointing_same_gradient(tmp_path):
+    blocks = configs.blast(48, 40)
+    p = Params.from_blocks(blocks)
+    g = Grid.from_athinput(write_athinput(tmp_path / "athinput", blocks), "blast")
+    n = 30
+    J0, g0, st0 = g.adjoint_gradient(n)
+    assert st0["snapshots"] == n + 1 and st0["tape_mode"] == 1 and st0["advances"] == 0
+    pitch = (48 + 8 + 15) // 16 * 16
+    state_bytes = 11 * 8 * pitch * (40 + 8)   # one snapshot (11 planes, rows of `pitch` doubles)
+    J, g1, st = g.adjoint_gradient(n, snapshot_bytes=(n + 1) * state_bytes)   # states only
+    assert st["tape_mode"] == 0 and st["advances"] == n and st["taped"] == n
+    assert J == J0 and np.array_equal(g1, g0)
+    for slots in (3, 6):
+        J, g1, st = g.adjoint_gradient(n, snapshot_bytes=slots * state_bytes)
+        assert st["snapshots"] <= slots and st["advances"] > n
+        assert J == J0 and np.array_equal(g1, g0), slots
+    g.close()
+    assert p is not None
+
+
+# ---------------------------------------------------------------------------
+# the adjoint configuration: field loop 256 x 256, 200 steps
+# ---------------------------------------------------------------------------
+NX, NSTEPS, SEED = 256, 200, 2024
+
+
+def _field_loop_case(tmp_path):
+    blocks = configs.field_loop(NX, NX)
+    blocks["time"]["nlim"] = NSTEPS
+    ath = write_athinput(tmp_path / "athinput", blocks)
+    base = problem_state("field_loop", Params(ath))
+    rho = fl.smoothed_density(NX, NX, SEED)
+    return ath, base, rho
+
+
+def test_field_loop_256_dot_product(tmp_path):
+    ath, base, rho = _field_loop_case(tmp_path)
+    S0 = fl.density_state(base, rho)
+    g = Grid.from_athinput(ath, "field_loop")
+    g.upload(S0)
+    J, grad, st = g.adjoint_gradient(NSTEPS)
+    assert st["steps"] == NSTEPS
+    grho = fl.density_gradient(base, grad)
+    rng = np.random.default_rng(7)
+    for k in range(3):
+        drho = fl.smoothed_density(NX, NX, 100 + k, amp=1.0) - 1.0
+        Jt, dJ = g.tlm(NSTEPS, fl.density_direction(base, drho))
+        assert Jt == J
+        ip = float(np.sum(grho * drho))
+        # relative to the terms of the sum (dJ itself cancels); 200 steps of
+        # the linearised loop carry rounding at ~1e-10 of them (the same on
+        # the CPU build of this code)
+        scale = float(np.sum(np.abs(grho * drho)))
+        assert abs(ip - dJ) <= 1e-8 * scale, (k, ip, dJ, scale)
+    d = ah.interior_direction(rng, Params(ath).config())   # every plane at once
+    _, dJ = g.tlm(NSTEPS, d)
+    ip = float(np.sum(grad * d))
+    assert abs(ip - dJ) <= 1e-8 * float(np.sum(np.abs(grad * d))), (ip, dJ)
+    assert st["tape_mode"] == 1   # 256^2 x 200: every step's tape fits in HBM
+    g.close()
+
+
+@pytest.mark.slow
+def test_field_loop_256_finite_differences_of_reference(tmp_path):
+    """Central differences of the reference CPU path (32 runs of 200 steps,
+    in parallel) along 16 seeded smooth density directions."""
+    if not refutil.have_ref("file", "roe"):
+        pytest.skip("oracle/_ref not built")
+    ath, base, rho = _field_loop_case(tmp_path)
+    S0 = fl.density_state(base, rho)
+    g = Grid.from_athinput(ath, "field_loop")
+    g.upload(S0)
+    J, grad, _ = g.adjoint_gradient(NSTEPS)
+    g.close()
+    grho = fl.density_gradient(base, grad)
+    eps = 1e-6
+    dirs = [fl.smoothed_density(NX, NX, 1000 + k, amp=1.0) - 1.0 for k in range(16)]
+    procs = []
+    for k, drho in enumerate(dirs):
+        for s, tag in ((1.0, "p"), (-1.0, "m")):
+            init = refutil.write_raw(tmp_path / f"init_{k}{tag}.bin", fl.density_state(base, rho + s * eps * drho))
+            out = tmp_path / f"out_{k}{tag}.bin"
+            cmd = [str(refutil.ref_binary("file", "roe")), "-i", str(ath), "--init", str(init), "--dump", str(out)]
+            procs.append((k, tag, out, subprocess.Popen(cmd, cwd=tmp_path, stdout=subprocess.DEVNULL,
+                                                         stderr=subprocess.PIPE)))
+    Jv = {}
+    for k, tag, out, p in procs:
+        _, err = p.communicate(timeout=1800)
+        assert p.returncode == 0, err.decode()[-1000:]
+        r = refutil.read_raw(out)
+        assert r["nstep"] == NSTEPS
+        Jv[(k, tag)] = fl.objective(r["planes"])
+    rows = []
+    for k, drho in enumerate(dirs):
+        fd = (Jv[(k, "p")] - Jv[(k, "m")]) / (2 * eps)
+        ad = float(np.sum(grho * drho))
+        rows.append((k, fd, ad, abs(fd - ad) / abs(ad)))
+    report = "\n".join(f"direction {k:2d}: fd {fd:+.12e} adjoint {ad:+.12e} rel {e:.2e}" for k, fd, ad, e in rows)
+    print(report)
+    out = Path("gpurun_out") if Path("gpurun_out").is_dir() else Path(tempfile.gettempdir())
+    (out / "athb_fd_report.txt").write_text(report + "\n")
+    assert sorted(e for _, _, _, e in rows)[len(rows) // 2] <= 1e-2, report
+
+
+def test_torch_autograd_function(tmp_path):
+    """dJ/drho through a torch.autograd.Function that calls the C ABI."""
+    torch = pytest.importorskip("torch")
+    blocks = configs.field_loop(32, 32)
+    ath = write_athinput(tmp_path / "athinput", blocks)
+    base = problem_state("field_loop", Params(ath))
+    g = Grid.from_athinput(ath, "field_loop")
+    n = 20
+
+    class MagneticEnergy(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, rho):
+            g.upload(fl.density_state(base, rho.detach().cpu().numpy()))
+            J, grad, _ = g.adjoint_gradient(n)
+            ctx.save_for_backward(torch.from_numpy(fl.density_gradient(base, grad)))
+            return torch.tensor(J, dtype=torch.float64)
+
+        @staticmethod
+        def backward(ctx, gJ):
+            (gr,) = ctx.saved_tensors
+            return gJ * gr
+
+    rho = torch.tensor(fl.smoothed_density(32, 32, 3), dtype=torch.float64, requires_grad=True)
+    J = MagneticEnergy.apply(rho)
+    (2.0 * J).backward()
+    drho = fl.smoothed_density(32, 32, 4, amp=1.0) - 1.0
+    g.upload(fl.density_state(base, rho.detach().numpy()))
+    _, dJ = g.tlm(n, fl.density_direction(base, drho))
+    assert abs(float(torch.sum(rho.grad * torch.from_numpy(drho))) - 2.0 * dJ) <= 1e-10 * abs(2.0 * dJ)
+    g.close()

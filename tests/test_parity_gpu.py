@@ -59,37 +59,6 @@ def test_step_bit_exact(name, tmp_path):
     _compare(ref, planes, dt, t, n)
 
 
-def _random_state(rng, nx1, nx2, smooth: bool) -> np.ndarray:
-    """A random, divergence-free, positive state (periodic) in the raw layout."""
-    sx, sy = nx1 + 8, nx2 + 8
-    P = np.zeros((11, sy, sx))
-
-    def field(lo, hi):
-        x = rng.uniform(lo, hi, size=(sy, sx))
-        if smooth:
-            for _ in range(4):
-                x = 0.25 * (np.roll(x, 1, 0) + np.roll(x, -1, 0) + np.roll(x, 1, 1) + np.roll(x, -1, 1))
-        return x
-
-    d = field(0.3, 2.0)
-    v1, v2, v3 = field(-1.5, 1.5), field(-1.5, 1.5), field(-0.5, 0.5)
-    p = field(0.02, 1.0)
-    # face fields from a vector potential so that div B = 0 to round-off
-    az = field(-0.05, 0.05)
-    b1i = np.zeros((sy, sx)); b2i = np.zeros((sy, sx))
-    b1i[:-1, :] = (az[1:, :] - az[:-1, :]) * 20.0
-    b2i[:, :-1] = -(az[:, 1:] - az[:, :-1]) * 20.0
-    b3i = field(-0.3, 0.3)
-    b1c = np.zeros((sy, sx)); b2c = np.zeros((sy, sx))
-    b1c[:, :-1] = 0.5 * (b1i[:, :-1] + b1i[:, 1:])
-    b2c[:-1, :] = 0.5 * (b2i[:-1, :] + b2i[1:, :])
-    g1 = configs.GAMMA - 1.0
-    e = p / g1 + 0.5 * d * (v1 * v1 + v2 * v2 + v3 * v3) + 0.5 * (b1c * b1c + b2c * b2c + b3i * b3i)
-    for k, a in enumerate([d, d * v1, d * v2, d * v3, e, b1c, b2c, b3i, b1i, b2i, b3i]):
-        P[k] = a
-    return P
-
-
 @pytest.mark.parametrize("smooth", [True, False])
 @pytest.mark.parametrize("flux", ["roe", "hlle"])
 def test_random_states_bit_exact(smooth, flux, tmp_path):
@@ -99,7 +68,7 @@ def test_random_states_bit_exact(smooth, flux, tmp_path):
         pytest.skip("oracle/_ref not built")
     rng = np.random.default_rng(1234 + smooth)
     nx1, nx2 = 40, 28
-    P = _random_state(rng, nx1, nx2, smooth)
+    P = refutil.random_state(rng, nx1, nx2, smooth)
     blocks = configs.field_loop(nx1, nx2, flux=flux)
     blocks["time"]["nlim"] = 6
     ath = write_athinput(tmp_path / "athinput", blocks)
