@@ -40,7 +40,7 @@ def _setup_signatures():
         "integrate_2d": [gp], "lr_states_init": [C.c_int, C.c_int], "lr_states_destruct": [],
         "set_bvals_init": [gp], "set_bvals": [gp, C.c_int], "new_dt": [gp],
         "athb_dropin_set_bc": [C.c_int] * 4, "athb_dropin_set_flux": [C.c_int],
-        "athb_dropin_set_device": [C.c_int],
+        "athb_dropin_set_device": [C.c_int], "athb_dropin_set_host_unchanged": [C.c_int],
         "athb_dropin_bytes": [C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)],
     }.items():
         f = getattr(L, name)
@@ -116,9 +116,11 @@ class DropInLoop:
     """The reference main loop on a HostGrid through the drop-in ABI."""
 
     def __init__(self, hg: HostGrid, gamma: float, cour_no: float, bc=(4, 4, 4, 4), flux: int = 0,
-                 device: int = 0):
+                 device: int = 0, host_unchanged: bool = False):
         self.L = _setup_signatures()
         self.L.athb_dropin_set_device(device)
+        # the loop below never writes the Grid between the drop-in calls
+        self.L.athb_dropin_set_host_unchanged(int(host_unchanged))
         self.hg = hg
         C.c_double.in_dll(self.L, "Gamma").value = gamma
         C.c_double.in_dll(self.L, "Gamma_1").value = gamma - 1.0

@@ -235,11 +235,18 @@ class ClockSampler:
             self.path = Path(tempfile.mkstemp(suffix=".csv")[1])
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "20"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            # the timed region can be shorter than nvidia-smi's start-up: wait
+            # for its first sample so that the region is covered
+            t0 = time.time()
+            while time.time() - t0 < 10.0 and self.path.stat().st_size == 0 and self.proc.poll() is None:
+                time.sleep(0.01)
+            self.skip = len(self.path.read_text().splitlines())
         return self
 
     def __exit__(self, *exc):
         if self.proc:
+            time.sleep(0.05)   # a sample just after the region
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -251,7 +258,10 @@ class ClockSampler:
             return None
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.path.read_text().splitlines():
+        lines = self.path.read_text().splitlines()
+        # samples from the last one before the region on (the region itself
+        # may be shorter than the sampling interval)
+        for line in lines[max(0, getattr(self, "skip", 1) - 1):]:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
@@ -361,7 +371,8 @@ def ours(a) -> None:
             "clocks": clk.summary()}
 
     if not a.no_e2e:
-        line["e2e"] = e2e(a, ath, local, ws)  # every rank: a collective for N > 1
+        line["e2e"] = e2e(a, ath, local, ws, host_unchanged=True)  # every rank: a collective for N > 1
+        line["e2e_default_mode"] = e2e(a, ath, local, ws, host_unchanged=False)
     if rank == 0 and ws == 1 and not a.no_cpu and ref_exe().exists():
         r = run_ref_sample(ath, a.cpu_steps, 1, td)
         line["cpu_baseline"] = {"value": r["value"], "unit": UNIT, "cores": 1, "kind": "reference",
@@ -373,11 +384,16 @@ def ours(a) -> None:
         torch.distributed.destroy_process_group()
 
 
-def e2e(a, ath: Path, device: int = 0, ws: int = 1) -> dict:
-    """The same metric through the reference-named drop-in ABI: the host Grid
-    (pinned) is the state; every step copies it to the GPU and the result back.
-    With ws ranks each runs its own replica on its GPU (collective: the
-    whole-job value uses the slowest rank's time)."""
+def e2e(a, ath: Path, device: int = 0, ws: int = 1, host_unchanged: bool = True) -> dict:
+    """The same metric through the reference-named drop-in ABI: the reference
+    main loop (integrate_2d, new_dt, set_bvals) on a pinned host Grid, which
+    after every call holds exactly what the reference's would.
+    host_unchanged: the opt-in mode for loops that do not write the Grid
+    between calls (athb_dropin_set_host_unchanged): the device copy stays
+    authoritative, so a step uploads nothing and downloads the cells it writes
+    plus the ghost frame; otherwise every call uploads what it reads.  With ws
+    ranks each runs its own replica on its GPU (collective: the whole-job
+    value uses the slowest rank's time)."""
     from athena_cuda_b200 import Params, configs, problem_state
     from athena_cuda_b200.dropin import DropInLoop, HostGrid
 
@@ -386,7 +402,8 @@ def e2e(a, ath: Path, device: int = 0, ws: int = 1) -> dict:
     planes = problem_state("field_loop", p)
     dx1, dx2 = (cfg.x1max - cfg.x1min) / cfg.nx1, (cfg.x2max - cfg.x2min) / cfg.nx2
     hg = HostGrid(planes, dx1, dx2, cfg.x1min, cfg.x2min)
-    loop = DropInLoop(hg, configs.GAMMA, cfg.cour_no, bc=(4, 4, 4, 4), device=device)
+    loop = DropInLoop(hg, configs.GAMMA, cfg.cour_no, bc=(4, 4, 4, 4), device=device,
+                      host_unchanged=host_unchanged)
     loop.steps(2)  # warm-up
     h0, d0 = loop.bytes_moved()
     t0 = time.perf_counter()
@@ -398,9 +415,12 @@ def e2e(a, ath: Path, device: int = 0, ws: int = 1) -> dict:
     if ws > 1:
         import torch
         dt = max_over_ranks(dt, ws, torch.device("cuda", device))
+    path = "integrate_2d + new_dt + set_bvals drop-in calls on a pinned host Grid"
+    if host_unchanged:
+        path += (" (host-unchanged mode: the device copy is authoritative; per step the cells integrate_2d "
+                 "writes and the ghost frame come down, nothing goes up)")
     return {"value": ws * a.nx * a.ny * n / dt, "unit": UNIT, "h2d_bytes_per_step": (h1 - h0) // n,
-            "d2h_bytes_per_step": (d1 - d0) // n, "steps": n,
-            "path": "integrate_2d + new_dt + set_bvals drop-in calls on a pinned host Grid"}
+            "d2h_bytes_per_step": (d1 - d0) // n, "steps": n, "path": path}
 
 
 def _time_ly(g, ly: int) -> float:

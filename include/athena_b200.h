@@ -362,6 +362,15 @@ void athb_dropin_set_bc(int ibc_x1, int obc_x1, int ibc_x2, int obc_x2);
  * ATHB_DEVICE environment variable, else 0).                                */
 void athb_dropin_set_device(int device);
 void athb_dropin_set_flux(int flux);
+/* Opt-in for programs that do not modify the Grid between the drop-in calls
+ * (the reference main loop between outputs, src/main.c:229-307): after the
+ * first full upload the device copy is authoritative, integrate_2d uploads
+ * nothing and new_dt reuses the CFL max its step already reduced; every call
+ * still leaves the host Grid exactly as the reference would (integrate_2d
+ * downloads the cells it writes, set_bvals the ghost frame).  Default off;
+ * the environment variable ATHB_DROPIN_HOST_UNCHANGED=1 turns it on.  A
+ * caller that writes the Grid must call this again (with 0 or 1) first.     */
+void athb_dropin_set_host_unchanged(int on);
 /* Bytes the drop-in entry points have copied host->device / device->host.  */
 void athb_dropin_bytes(unsigned long long *h2d, unsigned long long *d2h);
 

@@ -47,8 +47,28 @@ def test_linked_dropin_binary_bit_exact(name, tmp_path):
     assert (got["nstep"], got["time"], got["dt"]) == (ref["nstep"], ref["time"], ref["dt"])
 
 
+@pytest.mark.parametrize("name", ["blast_40x60", "blast_reflect_mixed", "field_loop_64x32", "cpaw2d_32x16_period",
+                                  "userbc_inflow_40x30"])
+def test_linked_dropin_binary_host_unchanged_mode(name, tmp_path, monkeypatch):
+    """The reference's own driver, relinked, with the opt-in host-unchanged
+    mode (ATHB_DROPIN_HOST_UNCHANGED=1): same output bit for bit; user
+    boundary functions fall back to the full path."""
+    problem, blocks, steps = CASES[name]
+    drop = refutil.REF_DIR / f"athdrop_{problem}"
+    if not (drop.exists() and refutil.have_ref(problem)):
+        pytest.skip("oracle/_ref drop-in builds missing (python oracle/build_ref.py)")
+    ath = write_athinput(tmp_path / "athinput", blocks)
+    ref = refutil.run_ref(problem, "roe", ath, tmp_path, steps=steps)
+    monkeypatch.setenv("ATHB_DROPIN_HOST_UNCHANGED", "1")
+    got = refutil.run_ref(problem, "roe", ath, tmp_path, steps=steps, exe=drop)
+    rep = refutil.mismatch_report(ref["planes"], got["planes"], PLANES)
+    assert rep == "", rep
+    assert (got["nstep"], got["time"], got["dt"]) == (ref["nstep"], ref["time"], ref["dt"])
+
+
+@pytest.mark.parametrize("host_unchanged", [False, True])
 @pytest.mark.parametrize("name", ["blast_40x60", "blast_reflect_mixed", "field_loop_64x32"])
-def test_python_dropin_loop_bit_exact(name, tmp_path):
+def test_python_dropin_loop_bit_exact(name, host_unchanged, tmp_path):
     problem, blocks, steps = CASES[name]
     if not refutil.have_ref(problem):
         pytest.skip("oracle/_ref not built")
@@ -58,12 +78,18 @@ def test_python_dropin_loop_bit_exact(name, tmp_path):
     cfg = p.config()
     hg = HostGrid(problem_state(problem, p), (cfg.x1max - cfg.x1min) / cfg.nx1,
                   (cfg.x2max - cfg.x2min) / cfg.nx2, cfg.x1min, cfg.x2min)
-    loop = DropInLoop(hg, configs.GAMMA, cfg.cour_no, bc=(cfg.bc_ix1, cfg.bc_ox1, cfg.bc_ix2, cfg.bc_ox2))
+    loop = DropInLoop(hg, configs.GAMMA, cfg.cour_no, bc=(cfg.bc_ix1, cfg.bc_ox1, cfg.bc_ix2, cfg.bc_ox2),
+                      host_unchanged=host_unchanged)
+    h_entry, _ = loop.bytes_moved()   # the counters run for the whole process
     loop.steps(steps, tlim=cfg.tlim)
+    h2d = loop.bytes_moved()[0] - h_entry
     got = hg.planes()
     G = hg.grid
     loop.close()
     rep = refutil.mismatch_report(ref["planes"], got, PLANES)
     assert rep == "", rep
     assert (G.nstep, G.time, G.dt) == (ref["nstep"], ref["time"], ref["dt"])
+    if host_unchanged:   # one full upload by the first step, none after it
+        state = 8 * 11 * hg.sx * hg.sy
+        assert h2d <= state, (h2d, state)
     hg.close()
