@@ -43,6 +43,12 @@ class AdjointStats(C.Structure):
                 ("workspace_bytes", C.c_longlong), ("seconds", C.c_double), ("tape_mode", C.c_int)]
 
 
+class PpmOpts(C.Structure):
+    _fields_ = [("expr", C.c_char_p), ("usr_expr", C.c_int), ("nx1", C.c_int), ("nx2", C.c_int),
+                ("rgb", C.POINTER(C.c_float)), ("sdmin", C.c_int), ("sdmax", C.c_int),
+                ("dmin", C.c_float), ("dmax", C.c_float), ("num", C.c_int)]
+
+
 class GridInfo(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("nx1", "nx2", "sx", "sy", "is_", "ie", "js", "je")] + [
         (n, C.c_double) for n in ("dx1", "dx2", "x1_0", "x2_0")] + [
@@ -107,9 +113,13 @@ def lib() -> C.CDLL:
             "athb_batch_mode": (I, [P]),
             "athb_batch_generate": (I, [P, I, C.c_char_p, P]),
             "athb_generate": (I, [P, C.c_char_p, P]),
+            "athb_generate_device": (I, [P, C.c_char_p, P]),
             "athb_set_pause": (I, [P, D, I]),
             "athb_dump_bin": (I, [P, C.c_char_p]),
             "athb_dump_tab": (I, [P, C.c_char_p, C.c_char_p]),
+            "athb_output_ppm": (I, [P, C.c_char_p, C.POINTER(PpmOpts), C.POINTER(C.c_float),
+                                    C.POINTER(C.c_float)]),
+            "athb_palette_load": (I, [C.c_char_p, C.c_char_p, C.POINTER(C.c_float)]),
             "athb_profile_steps": (I, [P, I, dp]),
             "athb_fp64_peak": (I, [I, dp]),
             "athb_set_ly": (I, [P, I]),
@@ -135,7 +145,9 @@ def _dp(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
-# problem generators with a device form (athb_generate / athb_batch_generate)
+# problem generators whose device form is bit-identical to the host one
+# (athb_generate forms these on the GPU); cpaw2d also has a device form
+# (athb_generate_device, athb_batch_generate) equal to a few ulp
 DEVICE_PROBLEMS = ("blast", "field_loop")
 
 
@@ -323,6 +335,11 @@ class Grid:
         reset, no ghost fill); blast and field_loop are formed on the GPU."""
         _check(lib().athb_generate(self._h, name.encode(), params._h))
 
+    def generate_device(self, name: str, params: "Params") -> None:
+        """As generate, every built-in problem formed on the GPU (cpaw2d with
+        CUDA's sin/cos: a few ulp from the host generator)."""
+        _check(lib().athb_generate_device(self._h, name.encode(), params._h))
+
     def set_pause(self, tpause: float, on: bool = True) -> None:
         """Stop the device loop at the first step starting at time >= tpause."""
         _check(lib().athb_set_pause(self._h, tpause, int(on)))
@@ -335,6 +352,22 @@ class Grid:
         """The reference's table dump of the current state (src/dump_tab.c)."""
         _check(lib().athb_dump_tab(self._h, str(path).encode(), dat_fmt.encode() if dat_fmt else None))
 
+    def output_ppm(self, path, expr: str, usr_expr: bool = False, rgb: np.ndarray | None = None,
+                   dmin: float | None = None, dmax: float | None = None, num: int = 0,
+                   extremes: tuple[float, float] = (0.0, 0.0)) -> tuple[float, float]:
+        """The reference's ppm image of one expression (src/output_ppm.c);
+        returns the running (gmin, gmax), `extremes` being the previous ones
+        (ignored when num is 0)."""
+        o = PpmOpts(expr=expr.encode(), usr_expr=int(usr_expr), sdmin=int(dmin is not None),
+                    sdmax=int(dmax is not None), dmin=dmin or 0.0, dmax=dmax or 0.0, num=num)
+        if rgb is not None:
+            rgb = np.ascontiguousarray(rgb, dtype=np.float32)
+            assert rgb.size == 768
+            o.rgb = rgb.ctypes.data_as(C.POINTER(C.c_float))
+        gmin, gmax = C.c_float(extremes[0]), C.c_float(extremes[1])
+        _check(lib().athb_output_ppm(self._h, str(path).encode(), C.byref(o), C.byref(gmin), C.byref(gmax)))
+        return gmin.value, gmax.value
+
     def close(self) -> None:
         if self._h:
             lib().athb_destroy(self._h)
@@ -345,6 +378,14 @@ class Grid:
             self.close()
         except Exception:
             pass
+
+
+def load_palette(path, name: str) -> np.ndarray:
+    """Colour table `name` (256 x 3 floats in 0..1) from a palette file: the
+    reference's palette.h, or lines "<name> v0 .. v767"."""
+    rgb = np.zeros(768, dtype=np.float32)
+    _check(lib().athb_palette_load(str(path).encode(), name.encode(), rgb.ctypes.data_as(C.POINTER(C.c_float))))
+    return rgb
 
 
 def athinput_text(blocks: dict) -> str:
@@ -391,7 +432,8 @@ class Batch:
         return b
 
     def generate(self, k: int, name: str, params: "Params") -> None:
-        """Instance k's initial condition formed on the GPU (DEVICE_PROBLEMS)."""
+        """Instance k's initial condition formed on the GPU (built-in
+        problems, as Grid.generate_device)."""
         _check(lib().athb_batch_generate(self._h, k, name.encode(), params._h))
 
     def upload(self, k: int, planes: np.ndarray, dt=0.0, time=0.0, nstep=0) -> None:
@@ -440,8 +482,9 @@ class Batch:
 
     @property
     def mode(self) -> int:
-        """Batch.PERSISTENT (one cooperative launch per step) or Batch.PHASED
-        (one launch per phase); results are identical."""
+        """Batch.PHASED (one launch per phase, the default) or
+        Batch.PERSISTENT (one cooperative launch per step); results are
+        identical."""
         return lib().athb_batch_mode(self._h)
 
     @mode.setter

@@ -1,5 +1,6 @@
 // athb_batch.cu -- many independent grids of uneven size, each with its own
-// dt and end time, advanced by ONE persistent kernel launch per step.
+// dt and end time, advanced together: one launch per phase of the step for
+// all instances (the default), or ONE persistent kernel launch per step.
 //
 // The persistent kernel walks six phases (predict, half-step corner EMF,
 // correct, full-step corner EMF, update + CFL, ghost fill + finalize); in each
@@ -345,7 +346,7 @@ struct athb_batch {
   int* err = nullptr;
   unsigned long long* timing = nullptr;  // per-phase ns (when enabled), then a stamp
   bool timing_on = false;
-  int mode = ATHB_BATCH_PERSISTENT;
+  int mode = ATHB_BATCH_PHASED;
   int phase_total[kPhases] = {0, 0, 0, 0, 0, 0};  // work items per phase (active set)
   cudaStream_t stream = nullptr;
   int grid = 0;            // persistent blocks
@@ -626,7 +627,7 @@ extern "C" int athb_batch_generate(athb_batch* b, int k, const char* name, const
   if (!b || k < 0 || k >= b->n || !name || !p) return athb_fail(ATHB_ERR_ARG, "bad arguments");
   CUDA_TRY(cudaSetDevice(b->device));
   const int kind = athb_builtin_problem(name);
-  if (kind != kProblemBlast && kind != kProblemFieldLoop)
+  if (kind == kProblemNone)
     return athb_fail(ATHB_ERR_NOTFOUND, "problem \"%s\" has no device generator (use athb_batch_upload)", name);
   const InstGeom& I = b->geom[k];
   double* dst = nullptr;

@@ -162,6 +162,7 @@ extern "C" void athb_destroy(athb_ctx* c) {
   cudaFree(c->scr);
   cudaFree(c->st);
   cudaFree(c->aos);
+  cudaFree(c->cpaw_soln);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }

@@ -26,9 +26,9 @@ struct athb_ctx {
   // drop-in staging: AoS copy of the host Gas array
   void* aos = nullptr;
   size_t aos_bytes = 0;
-  // cpaw2d reference solution (host copy of the initial cell-centred state)
+  // cpaw2d reference solution: planes d .. B3c of the initial state, kept on
+  // the device in the state layout (stride ps, row pitch)
   double* cpaw_soln = nullptr;
-  ~athb_ctx() { delete[] cpaw_soln; }
 };
 
 // internal helpers (athb_core.cu)
@@ -49,3 +49,10 @@ int athb_builtin_problem(const char* name);  // kind of the registered generator
 int athb_generate_host(athb_ctx* c, const char* name, const athb_params* p);
 int athb_generate_device_into(int kind, const athb_params* p, double* state, double* az, long long ps, int pitch,
                               const athb_config& cfg, cudaStream_t stream);
+// the wave of the cpaw2d problem (src/cpaw2d.c:56-120), host libm
+struct athb_cpaw_wave {
+  double sin_a, cos_a, k_par, b_par, b_perp, v_par, v_perp, pres, den;
+};
+int athb_cpaw2d_wave(const athb_params* p, int nx1, int nx2, double dx1, double dx2, athb_cpaw_wave* w);
+// copy the current state's planes d .. B3c into c->cpaw_soln (allocated once)
+int athb_keep_cpaw_soln(athb_ctx* c);

@@ -140,35 +140,10 @@ struct Cpaw {
 int problem_cpaw2d(const athb_grid_info* gi, const athb_params* p, double* planes, void*) {
   View v{*gi, planes};
   const athb_grid_info& g = *gi;
-  double angle, b_par, b_perp, pres, v_par;
-  if (getd(p, "problem", "angle", &angle) || getd(p, "problem", "b_par", &b_par) ||
-      getd(p, "problem", "b_perp", &b_perp) || getd(p, "problem", "pres", &pres) ||
-      getd(p, "problem", "v_par", &v_par))
-    return ATHB_ERR_PARSE;
-  Cpaw w;
-  double lambda;
-  if (angle == 0.0) {
-    w.sin_a = 0.0; w.cos_a = 1.0;
-    lambda = g.nx1 * g.dx1;
-  } else if (angle == 90.0) {
-    w.sin_a = 1.0; w.cos_a = 0.0;
-    lambda = g.nx2 * g.dx2;
-  } else {
-    if ((g.nx1 * g.dx1) == (g.nx2 * g.dx2)) {
-      w.cos_a = w.sin_a = sqrt(0.5);
-    } else {
-      angle = atan((double)(g.nx1 * g.dx1) / (g.nx2 * g.dx2));
-      w.sin_a = sin(angle);
-      w.cos_a = cos(angle);
-    }
-    if (w.cos_a >= w.sin_a) lambda = g.nx1 * g.dx1 * w.cos_a;
-    else lambda = g.nx2 * g.dx2 * w.sin_a;
-  }
-  w.k_par = 2.0 * kPi / lambda;
-  w.b_par = b_par;
-  const double den = 1.0;
-  w.b_perp = b_perp;
-  const double v_perp = b_perp / sqrt((double)den);
+  athb_cpaw_wave q;
+  if (athb_cpaw2d_wave(p, g.nx1, g.nx2, g.dx1, g.dx2, &q)) return ATHB_ERR_PARSE;
+  Cpaw w{q.sin_a, q.cos_a, q.b_par, q.b_perp, q.k_par};
+  const double den = q.den, v_par = q.v_par, v_perp = q.v_perp, b_perp = q.b_perp, pres = q.pres;
   const double dx1 = g.dx1, dx2 = g.dx2;
   for (int j = g.js; j <= g.je + 1; j++) {
     for (int i = g.is; i <= g.ie + 1; i++) {
@@ -218,6 +193,42 @@ std::map<std::string, Entry>& registry() {
 
 }  // namespace
 
+// The wave's scalars (src/cpaw2d.c:56-120): the direction of propagation
+// from the grid's aspect, the wavelength along it, and the amplitudes.
+int athb_cpaw2d_wave(const athb_params* p, int nx1, int nx2, double dx1, double dx2, athb_cpaw_wave* w) {
+  double angle, b_par, b_perp, pres, v_par;
+  if (getd(p, "problem", "angle", &angle) || getd(p, "problem", "b_par", &b_par) ||
+      getd(p, "problem", "b_perp", &b_perp) || getd(p, "problem", "pres", &pres) ||
+      getd(p, "problem", "v_par", &v_par))
+    return ATHB_ERR_PARSE;
+  double lambda;
+  if (angle == 0.0) {
+    w->sin_a = 0.0; w->cos_a = 1.0;
+    lambda = nx1 * dx1;
+  } else if (angle == 90.0) {
+    w->sin_a = 1.0; w->cos_a = 0.0;
+    lambda = nx2 * dx2;
+  } else {
+    if ((nx1 * dx1) == (nx2 * dx2)) {
+      w->cos_a = w->sin_a = sqrt(0.5);
+    } else {
+      angle = atan((double)(nx1 * dx1) / (nx2 * dx2));
+      w->sin_a = sin(angle);
+      w->cos_a = cos(angle);
+    }
+    if (w->cos_a >= w->sin_a) lambda = nx1 * dx1 * w->cos_a;
+    else lambda = nx2 * dx2 * w->sin_a;
+  }
+  w->k_par = 2.0 * kPi / lambda;
+  w->b_par = b_par;
+  w->den = 1.0;
+  w->b_perp = b_perp;
+  w->v_perp = b_perp / sqrt((double)w->den);
+  w->v_par = v_par;
+  w->pres = pres;
+  return ATHB_OK;
+}
+
 extern "C" int athb_register_problem(const char* name, athb_problem_fn fn, void* user) {
   if (!name || !fn) return athb_fail(ATHB_ERR_ARG, "null argument");
   registry()[name] = Entry{fn, user};
@@ -254,14 +265,10 @@ int athb_generate_host(athb_ctx* c, const char* name, const athb_params* p) {
   std::vector<double> planes((size_t)ATHB_NPLANES * gi.sx * gi.sy, 0.0);
   rc = athb_problem_generate(name, &gi, p, planes.data());
   if (rc) return rc;
-  if (athb_builtin_problem(name) == kProblemCpaw2d) {
-    // keep the initial cell-centred state: src/cpaw2d.c:160-180 (Soln)
-    const size_t n = (size_t)8 * gi.sx * gi.sy;
-    delete[] c->cpaw_soln;
-    c->cpaw_soln = new double[n];
-    memcpy(c->cpaw_soln, planes.data(), n * sizeof(double));
-  }
-  return athb_upload(c, planes.data(), 0.0, 0.0, 0);
+  rc = athb_upload(c, planes.data(), 0.0, 0.0, 0);
+  // keep the initial cell-centred state: src/cpaw2d.c:160-180 (Soln)
+  if (rc == ATHB_OK && athb_builtin_problem(name) == kProblemCpaw2d) rc = athb_keep_cpaw_soln(c);
+  return rc;
 }
 
 extern "C" int athb_create_from_athinput(const char* path, int noverride, const char* const* overrides,
@@ -283,30 +290,5 @@ extern "C" int athb_create_from_athinput(const char* path, int noverride, const 
   if (rc == ATHB_OK) rc = athb_new_dt(c, nullptr);
   if (rc) { athb_destroy(c); return rc; }
   *out = c;
-  return ATHB_OK;
-}
-
-// src/cpaw2d.c:222-302 (Userwork_after_loop), accumulated in the same order.
-extern "C" int athb_cpaw2d_errors(athb_ctx* c, double err[9]) {
-  if (!c || !err) return athb_fail(ATHB_ERR_ARG, "null argument");
-  if (!c->cpaw_soln) return athb_fail(ATHB_ERR_ARG, "context was not created by the cpaw2d problem");
-  athb_grid_info g;
-  athb_grid_info_of(c, &g);
-  std::vector<double> planes((size_t)ATHB_NPLANES * g.sx * g.sy);
-  int rc = athb_download(c, planes.data(), nullptr, nullptr, nullptr);
-  if (rc) return rc;
-  auto U = [&](int p, int j, int i) { return planes[((size_t)p * g.sy + j) * g.sx + i]; };
-  auto S = [&](int p, int j, int i) { return c->cpaw_soln[((size_t)p * g.sy + j) * g.sx + i]; };
-  double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // d M1 M2 M3 E B1c B2c B3c
-  for (int j = g.js; j <= g.je; j++)
-    for (int i = g.is; i <= g.ie; i++)
-      for (int k = 0; k < 8; k++) e[k] += fabs(U(k, j, i) - S(k, j, i));
-  double rms = e[D] * e[D] + e[M1] * e[M1] + e[M2] * e[M2] + e[M3] * e[M3];
-  rms += e[B1C] * e[B1C] + e[B2C] * e[B2C] + e[B3C] * e[B3C];
-  rms += e[E] * e[E];
-  const double n = (double)(g.nx1 * g.nx2);
-  err[0] = sqrt(rms) / n;
-  err[1] = e[D] / n; err[2] = e[M1] / n; err[3] = e[M2] / n; err[4] = e[M3] / n;
-  err[5] = e[E] / n; err[6] = e[B1C] / n; err[7] = e[B2C] / n; err[8] = e[B3C] / n;
   return ATHB_OK;
 }

@@ -430,11 +430,21 @@ def _time_ly(g, ly: int) -> float:
     return g.profile(2)["predict"]
 
 
+def _blast_big() -> dict:
+    from athena_cuda_b200 import configs
+
+    b = configs.blast(1024, 1024, tlim=10.0)
+    return b
+
+
 def ensemble_arm(a) -> None:
     """Batched ensemble (configs: 512 blast instances, sizes 64..512 per side,
-    per-instance parameters, each to its own t = 0.1): one persistent
-    cooperative launch per step for all instances, against the same instances
-    run one after another with the single-grid stepper."""
+    per-instance parameters, each to its own t = 0.1): one launch per phase
+    (or one persistent cooperative launch per step) for all instances, against
+    the same instances run one after another with the single-grid stepper,
+    and against the ideal time: the larger of (all zone-cycles at the best
+    single-grid per-cell rate, a 1024^2 blast grid) and the longest single
+    instance run alone (the chain of dependent steps no batching shortens)."""
     import torch
 
     from athena_cuda_b200 import Batch, Grid, Params, autotune, ensemble, problem_state
@@ -446,7 +456,7 @@ def ensemble_arm(a) -> None:
         return
     sizes = [(b["grid"]["Nx1"], b["grid"]["Nx2"]) for _, b in items]
     runs = {}
-    for mode_name, mode in (("persistent", Batch.PERSISTENT), ("phased", Batch.PHASED)):
+    for mode_name, mode in (("phased", Batch.PHASED), ("persistent", Batch.PERSISTENT)):
         t0 = time.perf_counter()
         batch = Batch.from_problems(items)
         batch.mode = mode
@@ -484,6 +494,7 @@ def ensemble_arm(a) -> None:
     # grid at a time from the host does
     stride = a.seq_sample if a.seq_sample > 0 else 1
     seq_s, seq_zc, checked, plain_s = 0.0, 0, 0, 0.0
+    longest_s = 0.0
     iso_ly = {}
     for k in range(0, len(items), stride):
         name, blocks = items[k]
@@ -503,7 +514,9 @@ def ensemble_arm(a) -> None:
         torch.cuda.synchronize()
         w = time.perf_counter()
         g.run(100000)
-        seq_s += time.perf_counter() - w
+        one_s = time.perf_counter() - w
+        seq_s += one_s
+        longest_s = max(longest_s, one_s)
         planes, dt, t, n = g.download()
         # (2) one step per call, host reads the clock every step
         g.upload(problem_state(name, p))
@@ -520,6 +533,24 @@ def ensemble_arm(a) -> None:
             checked += 1
         g.close()
     scale = 1.0 if stride == 1 else zc / seq_zc
+    # the best single-grid rate: a 1024^2 blast grid, best segment length,
+    # 20 steps of the CUDA-graph loop timed with events
+    p = Params.from_blocks(_blast_big())
+    g = Grid.create(p.config())
+    g.upload(problem_state("blast", p))
+    g.set_bvals()
+    g.new_dt()
+    g.ly = min(((ly, _time_ly(g, ly)) for ly in (4, 8, 16, 32)), key=lambda x: x[1])[0]
+    g.run(3)
+    big_stream = torch.cuda.ExternalStream(g.stream)
+    b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    b0.record(big_stream)
+    g.run_async(20)
+    b1.record(big_stream)
+    b1.synchronize()
+    best_rate = 1024 * 1024 * 20 / (b0.elapsed_time(b1) * 1e-3)
+    g.close()
+    ideal_s = max(zc / best_rate, longest_s)
     line = {"metric": "ensemble zone-cycles/s (512 blast instances to t=0.1, batched)",
             "value": zc / batched_s, "unit": UNIT, "n_gpus": 1, "dtype": "f64", "data": "synthetic (seeded blast ensemble)",
             "config": {"workload": f"blast ensemble n={len(items)} sizes 64..512 per side", "seed": 2024,
@@ -530,7 +561,11 @@ def ensemble_arm(a) -> None:
             "sequential_s": seq_s * scale, "sequential_zc_per_s": seq_zc / seq_s,
             "speedup_vs_sequential": (seq_s * scale) / batched_s,
             "sequential_plain_s": plain_s * scale, "speedup_vs_sequential_plain": (plain_s * scale) / batched_s,
-            "sequential_sample_stride": stride, "bit_exact_spot_checks": checked}
+            "sequential_sample_stride": stride, "bit_exact_spot_checks": checked,
+            "ideal": {"s": ideal_s, "best_single_grid_zc_per_s": best_rate, "work_bound_s": zc / best_rate,
+                      "longest_instance_s": longest_s if stride == 1 else None,
+                      "speedup_bound_vs_sequential_plain": (plain_s * scale) / ideal_s,
+                      "batched_over_ideal": batched_s / ideal_s}}
     ref = ROOT / "oracle" / "_ref" / "athref_blast_roe"
     if ref.exists():
         # the reference CPU path, one process per host core (up to 16, each

@@ -184,6 +184,29 @@ int athb_rows_put(athb_ctx *ctx, int j0, int nrows, const double *host);
 int athb_dump_bin(athb_ctx *ctx, const char *path);
 int athb_dump_tab(athb_ctx *ctx, const char *path, const char *dat_fmt);
 
+/* Single-variable ppm image of the resident state, the reference's
+ * output_ppm (src/output_ppm.c:37-143) of an expression of src/output.c
+ * (d M1 M2 M3 E B1c B2c B3c ME V1 V2 V3 P cs2 S) or, with usr_expr, of the
+ * field-loop problem's get_usr_expr (J3, Bp2; src/field_loop.c:161-179).
+ * The expression is evaluated on the GPU and only the float image comes
+ * down.  The image is the first nx1 x nx2 interior cells (0: the grid's),
+ * as the reference's subset2.  rgb: a 256x3 palette in 0..1 (NULL: black /
+ * white at dmax); sdmin/sdmax fix the scale.  gmin/gmax carry the running
+ * extremes between the outputs of one <output> block (num 0 resets them).   */
+typedef struct athb_ppm_opts {
+  const char *expr;
+  int usr_expr;
+  int nx1, nx2;
+  const float *rgb;
+  int sdmin, sdmax;
+  float dmin, dmax;
+  int num;                      /* output number (0: first image)           */
+} athb_ppm_opts;
+int athb_output_ppm(athb_ctx *ctx, const char *path, const athb_ppm_opts *opts, float *gmin, float *gmax);
+/* Palette `name` (256 x 3 floats) from a file of colour tables, either in
+ * the C form of the reference's palette.h or as lines "<name> v0 .. v767". */
+int athb_palette_load(const char *path, const char *name, float rgb[768]);
+
 /* Diagnostics of the resident state, computed on the GPU over the interior:
  * out[0] mass, out[1] total energy, out[2] magnetic energy (sum of
  * (B1c^2+B2c^2+B3c^2)/2 dV), out[3] sum of Bp2 = B1c^2+B2c^2 dV (the
@@ -235,6 +258,12 @@ int athb_problem_generate(const char *name, const athb_grid_info *g, const athb_
  * bit-identical to the host generators'); "cpaw2d" (libm sin/cos per cell)
  * and registered generators run on the host and are uploaded.               */
 int athb_generate(athb_ctx *ctx, const char *name, const athb_params *p);
+/* Every built-in generator on the GPU, "cpaw2d" included: its per-cell
+ * sin/cos are CUDA's (within 2 ulp of the exact values, where libm's are
+ * within 1), so the cpaw2d state agrees with athb_generate's to a few ulp of
+ * each term (face fields: of the vector potential over dx), not bit for bit.
+ * ATHB_ERR_NOTFOUND for registered (non-built-in) generators.               */
+int athb_generate_device(athb_ctx *ctx, const char *name, const athb_params *p);
 
 /* Parse an athinput file (+ overrides), create the context, run the problem
  * generator (athb_generate), set_bvals and the first new_dt: the state
@@ -244,7 +273,9 @@ int athb_create_from_athinput(const char *path, int noverride, const char *const
 
 /* cpaw2d L1 errors against the initial state (src/cpaw2d.c:222-302,
  * Userwork_after_loop): err[0]=RMS, err[1..8] = d M1 M2 M3 E B1c B2c B3c,
- * each divided by Nx1*Nx2.  Only for contexts created by cpaw2d.            */
+ * each divided by Nx1*Nx2.  Only for contexts created by cpaw2d.  The sums
+ * run on the GPU in the reference's order against the initial state kept on
+ * the device (8 doubles come back): equal to the reference's host loop.     */
 int athb_cpaw2d_errors(athb_ctx *ctx, double err[9]);
 
 /* ---- batched ensembles ---------------------------------------------------- */
@@ -258,8 +289,8 @@ int athb_batch_size(const athb_batch *b);
 /* instance state in the athb_upload layout, and its clock                   */
 int athb_batch_upload(athb_batch *b, int k, const double *planes, double dt, double time, int nstep);
 int athb_batch_download(athb_batch *b, int k, double *planes, double *dt, double *time, int *nstep);
-/* instance k's initial condition formed on the GPU (built-in "blast" and
- * "field_loop" only, see athb_generate), clock reset                        */
+/* instance k's initial condition formed on the GPU (built-in generators
+ * only, as athb_generate_device), clock reset                               */
 int athb_batch_generate(athb_batch *b, int k, const char *name, const athb_params *p);
 /* set_bvals and the first new_dt of every instance (src/main.c:139-149)      */
 int athb_batch_prepare(athb_batch *b);
@@ -280,8 +311,9 @@ int athb_batch_grid(const athb_batch *b);
  * device time stamps after each phase).  enable: 1 start recording (resets),
  * 0 stop, -1 leave as is; ms_out may be NULL.                              */
 int athb_batch_timing(athb_batch *b, int enable, double *ms_out);
-/* execution mode: one persistent cooperative launch per step (default), or
- * one launch per phase with the hardware block scheduler; identical results */
+/* execution mode: one launch per phase with the hardware block scheduler
+ * (default: each phase keeps its single-grid kernel's register budget), or
+ * one persistent cooperative launch per step; identical results             */
 #define ATHB_BATCH_PERSISTENT 0
 #define ATHB_BATCH_PHASED 1
 int athb_batch_set_mode(athb_batch *b, int mode);

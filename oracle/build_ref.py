@@ -17,6 +17,8 @@ Builds, per problem generator and flux:
   reference's host-side files (``init_grid.c``, ``par.c``, the problem file)
   linked against ``libathena_b200.so`` instead of the reference's integrator,
   boundary and dt sources -- the drop-in test (only when the library exists).
+* ``palettes.txt``: the colour tables of ``src/palette.h`` as text, written by
+  ``oracle/palette_dump.c`` (the palette file of the ppm parity tests).
 * ``athmain_{blast,field_loop,cpaw2d}``: the reference's own ``src/main.c``
   with its output code (``output.c``, ``dump_binary.c``, ``dump_tab.c`` ...),
   the program whose output files the command-line driver must reproduce;
@@ -117,6 +119,13 @@ def build(ref_root: Path = DEFAULT_REF, force: bool = False, lib: Path | None = 
                     ["-Dflux_roe=flux_hlle"], inc, force),
     }
     built = []
+    pal = OUT / "palettes.txt"
+    pexe = obj / "palette_dump"
+    if force or not _newer(pal, [HERE / "palette_dump.c", src / "palette.h", HERE / "build_ref.py"]):
+        _run(["gcc", *CFLAGS, *inc, str(HERE / "palette_dump.c"), "-o", str(pexe)])
+        r = subprocess.run([str(pexe)], capture_output=True, text=True, check=True)
+        pal.write_text(r.stdout)
+    built.append(pal)
     for prob, (pfile, pdefs) in PROBLEMS.items():
         harness = _cc(HERE / "ref_harness.c", obj / f"harness_{prob}.o", pdefs, inc, force)
         pobj = [] if pfile is None else [_cc(src / pfile, obj / f"prob_{prob}.o", pdefs, inc, force)]  # src / absolute = absolute

@@ -35,6 +35,15 @@ def write_raw(path, planes: np.ndarray, nstep=0, dt=0.0, time=0.0, dx=(0.0, 0.0)
     return Path(path)
 
 
+def reference_root() -> Path | None:
+    """The reference source tree ($ATHENA_REF, else ``reference`` beside the
+    repository), or None where it is absent (CPU-side checks only)."""
+    import os
+    env = os.environ.get("ATHENA_REF")
+    p = Path(env) if env else ROOT.parent / "reference"
+    return p if p.is_dir() else None
+
+
 def ref_binary(problem: str, flux: str = "roe") -> Path:
     return REF_DIR / f"athref_{problem}_{flux}"
 

@@ -81,6 +81,8 @@ def test_phased_mode_matches_persistent():
     """One launch per phase gives the same bits as the persistent kernel."""
     items = _items()
     want = Batch.from_problems(items)
+    assert want.mode == Batch.PHASED   # the default
+    want.mode = Batch.PERSISTENT
     want.run(10_000)
     ref = [want.download(k) for k in range(want.n)]
     want.close()

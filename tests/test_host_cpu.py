@@ -12,7 +12,8 @@ import numpy as np
 import pytest
 
 import refutil
-from athena_cuda_b200 import LIB_PATH, NGHOST, PLANES, AthbError, Params, configs, lib, problem_state, write_athinput
+from athena_cuda_b200 import (LIB_PATH, NGHOST, PLANES, AthbError, Params, configs, lib, load_palette, problem_state,
+                              write_athinput)
 
 ROOT = Path(__file__).resolve().parent.parent
 HEADER = ROOT / "include" / "athena_b200.h"
@@ -92,3 +93,32 @@ def test_problem_generator_matches_reference(problem, tmp_path):
     # face fields: interior plus the outer faces B1i(ie+1) and B2i(je+1)
     np.testing.assert_array_equal(mine[8][ng:sy - ng, ng:sx - ng + 1], ref[8][ng:sy - ng, ng:sx - ng + 1])
     np.testing.assert_array_equal(mine[9][ng:sy - ng + 1, ng:sx - ng], ref[9][ng:sy - ng + 1, ng:sx - ng])
+
+
+def test_palette_file_forms(tmp_path):
+    """Both palette file forms the ppm output reads: the C initialisers of the
+    reference's palette.h and one text line per table."""
+    vals = np.linspace(0.0, 1.0, 768).astype(np.float32)
+    c_form = tmp_path / "pal.h"
+    c_form.write_text("static float other[256*3] = { 1.0, 2.0 };\n"
+                      "static float mine[256*3] = {\n" + " , ".join(f"{v:.6e}" for v in vals) + " ,\n};\n")
+    got = load_palette(c_form, "mine")
+    np.testing.assert_array_equal(got, np.array([float(f"{v:.6e}") for v in vals]).astype(np.float32))
+    short = load_palette(c_form, "other")   # a short initialiser: the rest is zero
+    assert short[0] == 1.0 and short[1] == 2.0 and not short[2:].any()
+    lines = tmp_path / "pal.txt"
+    lines.write_text("mine " + " ".join(f"{v:.9g}" for v in vals) + "\n")
+    np.testing.assert_array_equal(load_palette(lines, "mine"), vals)
+    with pytest.raises(AthbError, match="not found"):
+        load_palette(lines, "min")
+
+
+def test_reference_palettes_as_text():
+    """oracle/_ref/palettes.txt (written from the reference's palette.h) reads
+    back as the tables the C compiler builds from palette.h itself."""
+    pal = refutil.REF_DIR / "palettes.txt"
+    h = refutil.reference_root() / "src" / "palette.h" if refutil.reference_root() else None
+    if not pal.exists() or h is None or not h.exists():
+        pytest.skip("reference palettes not available")
+    for name in ("rainbow", "jh_colors", "step8", "step32", "idl1", "idl2", "heat"):
+        np.testing.assert_array_equal(load_palette(pal, name), load_palette(h, name), err_msg=name)

@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 import refutil
-from athena_cuda_b200 import Grid, configs, write_athinput
+from athena_cuda_b200 import Grid, Params, configs, problem_state, write_athinput
 
 pytestmark = pytest.mark.gpu
 
@@ -67,6 +67,16 @@ def test_cpaw2d_second_order_and_reference_errors(tmp_path):
         g = Grid.from_athinput(ath, "cpaw2d")
         g.run(1_000_000)
         e = g.cpaw2d_errors()
+        # the device sums are the reference's serial row-major sums, bit for
+        # bit (np.cumsum adds left to right)
+        U = g.download()[0]
+        S0 = problem_state("cpaw2d", Params(ath))
+        n = nx1 * nx2
+        sums = [float(np.cumsum(np.abs(U[k, 4:-4, 4:-4] - S0[k, 4:-4, 4:-4]).ravel())[-1]) for k in range(8)]
+        rms = sums[0] ** 2 + sums[1] ** 2 + sums[2] ** 2 + sums[3] ** 2
+        rms += sums[5] ** 2 + sums[6] ** 2 + sums[7] ** 2
+        rms += sums[4] ** 2
+        assert [e[0]] + list(e[1:]) == [math.sqrt(rms) / n] + [x / n for x in sums]
         g.close()
         assert g is not None and e[0] > 0
         errs.append(e[0])
