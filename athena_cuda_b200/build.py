@@ -33,7 +33,7 @@ CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", f"-I{ROOT / 'inc
              f"-I{CUDA_HOME / 'include'}"]
 
 CU_SOURCES = ["athb_core.cu", "athb_dropin.cu", "athb_batch.cu", "athb_noalloc.cu", "athb_output.cu", "athb_adjoint.cu",
-              "athb_problems_dev.cu"]
+              "athb_problems_dev.cu", "athb_slab.cu"]
 CPP_SOURCES = ["athinput.cpp", "problems.cpp"]
 HEADERS = ["dual.cuh", "mhd_physics.cuh", "step_types.cuh", "step_kernels.cuh", "athb_internal.h", "mhd_adjoint.cuh",
            "step_generic.cuh", "step_adjoint.cuh", "adjoint_driver.cuh"]

@@ -16,13 +16,28 @@ global cell sizes, and runs every main-loop iteration (src/main.c:229-307) as
 5. the physical x2 boundaries at the global ends (mode 2, one side).
 
 So every rank's state equals the matching rows of the single grid bit for
-bit.  The rows travel through host memory over ``torch.distributed`` (gloo,
-or any backend that takes CPU tensors), one exchange per iteration; the
-reference itself has no multi-process grid (``MPI_SERIAL``).
+bit.  Three transports carry the rows and the maximum (the reference itself
+has no multi-process grid, ``MPI_SERIAL``):
+
+* ``host``: rows through host memory over ``torch.distributed`` (gloo, or any
+  backend that takes CPU tensors), the maximum as a CPU all-reduce;
+* ``nccl``: ranks on distinct GPUs; the rows packed on the GPU into device
+  buffers (``athb_rows_pack``), sent and received by NCCL on the grid's
+  stream and unpacked on the GPU, the maximum all-reduced by NCCL on a device
+  word (``athb_max_dti_bits_device`` / ``athb_finish_step_device``): no host
+  copy and no host synchronisation per iteration;
+* ``ipc``: ranks sharing a GPU (or peers): every rank's receive buffers and
+  maximum words live in one device allocation mapped by the other ranks
+  through CUDA IPC; a rank packs its rows and copies them with
+  ``cudaMemcpyAsync`` into its neighbours' receive buffers, writes its
+  maximum into rank 0's words, and two host barriers per iteration order the
+  copies (the buffers alternate between two parities, so a copy never lands
+  in a buffer its owner is still unpacking).
 """
 from __future__ import annotations
 
 import ctypes as C
+import time
 
 import numpy as np
 
@@ -78,20 +93,47 @@ def _sigs():
         ("athb_ghost_fill", I, [P, I, I]),
         ("athb_rows_get", I, [P, I, I, dp]),
         ("athb_rows_put", I, [P, I, I, dp]),
+        ("athb_rows_pack", I, [P, I, I, P]),
+        ("athb_rows_unpack", I, [P, I, I, P]),
+        ("athb_max_dti_bits_device", I, [P, P]),
+        ("athb_finish_step_device", I, [P, P, I, I]),
+        ("athb_device_alloc", P, [P, C.c_ulonglong]),
+        ("athb_device_free", None, [P, P]),
+        ("athb_ipc_handle", I, [P, P, C.c_char_p]),
+        ("athb_ipc_open", I, [P, C.c_char_p, C.POINTER(C.c_void_p)]),
+        ("athb_ipc_close", I, [P, P]),
+        ("athb_copy_async", I, [P, P, P, C.c_ulonglong]),
     ]:
         f = getattr(L, name)
         f.restype, f.argtypes = res, args
     _sigs_done = True
 
 
+MAX_RANKS = 64          # words of the ipc maximum board per parity
+BOARD_BYTES = 2 * MAX_RANKS * 8
+
+
 class SlabGrid:
     """This rank's slab of a grid given by athinput blocks; the process group
-    must be initialised (any backend that reduces and sends CPU tensors)."""
+    must be initialised: for transport "host" any backend that reduces and
+    sends CPU tensors, for "nccl" an NCCL group (one GPU per rank), for "ipc"
+    a group that gathers objects and has a barrier (gloo)."""
 
-    def __init__(self, blocks: dict, problem: str, rank: int, ranks: int, group=None):
+    TRANSPORTS = ("host", "nccl", "ipc")
+
+    def __init__(self, blocks: dict, problem: str, rank: int, ranks: int, group=None, transport: str = "host"):
         import torch.distributed as dist
 
         _sigs()
+        if transport not in self.TRANSPORTS:
+            raise ValueError(f"transport must be one of {self.TRANSPORTS}")
+        if transport == "ipc" and ranks > MAX_RANKS:
+            raise ValueError(f"ipc transport: at most {MAX_RANKS} ranks")
+        self.transport = transport
+        self.exchange_s = 0.0    # host time spent in the exchange and the maximum
+        self.iterations = 0
+        self.parity = 0          # ipc receive buffers in use (alternate per exchange)
+        self.bpar = 0            # ipc maximum board in use (alternate per step finish)
         self.dist, self.group, self.rank, self.ranks = dist, group, rank, ranks
         params = Params.from_blocks(blocks)
         gcfg = params.config()
@@ -114,9 +156,124 @@ class SlabGrid:
         # are refilled below)
         full = problem_state(problem, params)
         self.grid.upload(np.ascontiguousarray(full[:, self.j0:self.j0 + self.ny + 2 * NG, :]))
+        self.row_doubles = len(PLANES) * NG * self.sx
+        if transport == "nccl":
+            self._nccl_setup(gcfg.device)
+        elif transport == "ipc":
+            self._ipc_setup()
         self._ghosts()
         _check(lib().athb_cfl_local(self.grid._h))
-        _check(lib().athb_finish_step(self.grid._h, self._global_max(), 0))
+        self._finish(0)
+
+    # -- transports ----------------------------------------------------------
+    def _nccl_setup(self, device: int) -> None:
+        import torch
+
+        dev = torch.device("cuda", device)
+        self.tdev = dev
+        self.stream = torch.cuda.ExternalStream(self.grid.stream, device=dev)
+        self.dti = torch.zeros(1, dtype=torch.int64, device=dev)
+        self.sendbuf = {s: torch.empty(self.row_doubles, dtype=torch.float64, device=dev) for s in ("lo", "hi")}
+        self.recvbuf = {s: torch.empty(self.row_doubles, dtype=torch.float64, device=dev) for s in ("lo", "hi")}
+
+    def _ipc_setup(self) -> None:
+        L, h = lib(), self.grid._h
+        rb = self.row_doubles * 8
+        # one allocation per rank: the maximum board, then receive buffers
+        # [parity][side] (side 0: rows from the rank below -> my lower
+        # ghosts; side 1: rows from the rank above -> my upper ghosts)
+        self.own = L.athb_device_alloc(h, BOARD_BYTES + 4 * rb)
+        self.send = L.athb_device_alloc(h, 2 * rb)
+        if not self.own or not self.send:
+            raise RuntimeError("athb_device_alloc failed")
+        handle = C.create_string_buffer(64)
+        _check(L.athb_ipc_handle(h, C.c_void_p(self.own), handle))
+        handles = [None] * self.ranks
+        self.dist.all_gather_object(handles, bytes(handle.raw), group=self.group)
+        self.peer = {self.rank: self.own}
+        for r in {self.below, self.above, 0} - {None, self.rank}:
+            ptr = C.c_void_p()
+            _check(L.athb_ipc_open(h, handles[r], C.byref(ptr)))
+            self.peer[r] = ptr.value
+        self.rb = rb
+
+    def _recv_addr(self, r: int, parity: int, side: int) -> int:
+        return self.peer[r] + BOARD_BYTES + (2 * parity + side) * self.rb
+
+    def _barrier(self) -> None:
+        self.dist.barrier(group=self.group)
+
+    def _finish(self, after_step: int) -> None:
+        """The maximum of 1/dt over the ranks, then the dt rule (and the
+        time advance after a step) on every rank."""
+        t0 = time.perf_counter()
+        L, h = lib(), self.grid._h
+        if self.transport == "host":
+            _check(L.athb_finish_step(h, self._global_max(), after_step))
+        elif self.transport == "nccl":
+            import torch
+
+            _check(L.athb_max_dti_bits_device(h, C.c_void_p(self.dti.data_ptr())))
+            with torch.cuda.stream(self.stream):
+                if self.ranks > 1:
+                    self.dist.all_reduce(self.dti, op=self.dist.ReduceOp.MAX, group=self.group)
+                _check(L.athb_finish_step_device(h, C.c_void_p(self.dti.data_ptr()), 1, after_step))
+        else:
+            # the board alternates between two parities per call: a rank
+            # writes parity q only after every rank has passed the barrier of
+            # the previous call, which each enters after its read of parity q
+            # two calls back has completed
+            board = self.peer[0] + self.bpar * MAX_RANKS * 8
+            self.bpar ^= 1
+            _check(L.athb_max_dti_bits_device(h, C.c_void_p(board + 8 * self.rank)))
+            self.grid.synchronize()
+            self._barrier()   # every rank's word is on rank 0's board
+            _check(L.athb_finish_step_device(h, C.c_void_p(board), self.ranks, after_step))
+        self.exchange_s += time.perf_counter() - t0
+
+    def _exchange_device(self) -> None:
+        L, h = lib(), self.grid._h
+        js, je = NG, NG + self.ny - 1
+        if self.transport == "nccl":
+            import torch
+
+            if self.below is not None:
+                _check(L.athb_rows_pack(h, js, NG, C.c_void_p(self.sendbuf["lo"].data_ptr())))
+            if self.above is not None:
+                _check(L.athb_rows_pack(h, je - NG + 1, NG, C.c_void_p(self.sendbuf["hi"].data_ptr())))
+            with torch.cuda.stream(self.stream):
+                ops = []
+                if self.below is not None:
+                    ops.append(self.dist.P2POp(self.dist.isend, self.sendbuf["lo"], self.below, group=self.group))
+                    ops.append(self.dist.P2POp(self.dist.irecv, self.recvbuf["lo"], self.below, group=self.group))
+                if self.above is not None:
+                    ops.append(self.dist.P2POp(self.dist.isend, self.sendbuf["hi"], self.above, group=self.group))
+                    ops.append(self.dist.P2POp(self.dist.irecv, self.recvbuf["hi"], self.above, group=self.group))
+                for w in self.dist.batch_isend_irecv(ops):
+                    w.wait()   # the grid's stream waits for the transfers
+            if self.below is not None:
+                _check(L.athb_rows_unpack(h, js - NG, NG, C.c_void_p(self.recvbuf["lo"].data_ptr())))
+            if self.above is not None:
+                _check(L.athb_rows_unpack(h, je + 1, NG, C.c_void_p(self.recvbuf["hi"].data_ptr())))
+            return
+        # ipc: my lowest rows become the upper ghosts of the rank below (its
+        # side 1), my highest rows the lower ghosts of the rank above (its
+        # side 0)
+        q = self.parity
+        if self.below is not None:
+            _check(L.athb_rows_pack(h, js, NG, C.c_void_p(self.send)))
+            _check(L.athb_copy_async(h, C.c_void_p(self._recv_addr(self.below, q, 1)), C.c_void_p(self.send),
+                                     self.rb))
+        if self.above is not None:
+            _check(L.athb_rows_pack(h, je - NG + 1, NG, C.c_void_p(self.send + self.rb)))
+            _check(L.athb_copy_async(h, C.c_void_p(self._recv_addr(self.above, q, 0)), C.c_void_p(self.send + self.rb),
+                                     self.rb))
+        self.grid.synchronize()
+        self._barrier()   # every copy into my receive buffers has landed
+        if self.below is not None:
+            _check(L.athb_rows_unpack(h, js - NG, NG, C.c_void_p(self._recv_addr(self.rank, q, 0))))
+        if self.above is not None:
+            _check(L.athb_rows_unpack(h, je + 1, NG, C.c_void_p(self._recv_addr(self.rank, q, 1))))
 
     # -- pieces ------------------------------------------------------------
     def _global_max(self) -> int:
@@ -161,16 +318,24 @@ class SlabGrid:
 
     def _ghosts(self) -> None:
         _check(lib().athb_ghost_fill(self.grid._h, 1, 3))
-        self._exchange()
+        t0 = time.perf_counter()
+        if self.ranks > 1:
+            if self.transport == "host":
+                self._exchange()
+            else:
+                self._exchange_device()
+        self.exchange_s += time.perf_counter() - t0
         if self.sides2:
             _check(lib().athb_ghost_fill(self.grid._h, 2, self.sides2))
+        self.parity ^= 1   # the next exchange lands in the other buffers
 
     # -- public ------------------------------------------------------------
     def step(self) -> None:
         """One iteration of the main loop on every rank (collective)."""
         _check(lib().athb_integrate_local(self.grid._h))
-        _check(lib().athb_finish_step(self.grid._h, self._global_max(), 1))
+        self._finish(1)
         self._ghosts()
+        self.iterations += 1
 
     def status(self) -> dict:
         return self.grid.status()
@@ -202,4 +367,17 @@ class SlabGrid:
         return None
 
     def close(self) -> None:
+        """Release the transport's buffers (collective for "ipc": no rank
+        frees a buffer another may still write), then the grid."""
+        if self.transport == "ipc" and getattr(self, "own", None):
+            L, h = lib(), self.grid._h
+            self.grid.synchronize()
+            self._barrier()
+            for r, ptr in self.peer.items():
+                if r != self.rank:
+                    _check(L.athb_ipc_close(h, C.c_void_p(ptr)))
+            self._barrier()
+            L.athb_device_free(h, C.c_void_p(self.own))
+            L.athb_device_free(h, C.c_void_p(self.send))
+            self.own = None
         self.grid.close()

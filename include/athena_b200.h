@@ -174,6 +174,26 @@ int athb_finish_step(athb_ctx *ctx, unsigned long long max_dti_bits, int after_s
 int athb_ghost_fill(athb_ctx *ctx, int mode, int sides);
 int athb_rows_get(athb_ctx *ctx, int j0, int nrows, double *host);
 int athb_rows_put(athb_ctx *ctx, int j0, int nrows, const double *host);
+/* The same exchange on device buffers (no host copy per iteration): rows
+ * [j0, j0+nrows) of the 11 planes packed into / unpacked from a contiguous
+ * device buffer [plane][row][Nx1+8] by a kernel on the context's stream;
+ * the running max of 1/dt written to a device word, and the step finished
+ * with the max over n device words (after an NCCL all-reduce: n = 1; read
+ * through IPC mappings of every rank's word: n = ranks).                    */
+int athb_rows_pack(athb_ctx *ctx, int j0, int nrows, double *dev);
+int athb_rows_unpack(athb_ctx *ctx, int j0, int nrows, const double *dev);
+int athb_max_dti_bits_device(athb_ctx *ctx, unsigned long long *dev);
+int athb_finish_step_device(athb_ctx *ctx, const unsigned long long *dev_bits, int n, int after_step);
+/* Device buffers shared between processes: cudaMalloc'd (zeroed) on the
+ * context's device, a CUDA-IPC handle (64 bytes) for another process, which
+ * opens it as a device pointer; athb_copy_async copies on the context's
+ * stream (cudaMemcpyAsync, plain peer stores when dst is a mapping).        */
+void *athb_device_alloc(athb_ctx *ctx, unsigned long long bytes);
+void athb_device_free(athb_ctx *ctx, void *dev);
+int athb_ipc_handle(athb_ctx *ctx, void *dev, unsigned char handle[64]);
+int athb_ipc_open(athb_ctx *ctx, const unsigned char handle[64], void **dev);
+int athb_ipc_close(athb_ctx *ctx, void *dev);
+int athb_copy_async(athb_ctx *ctx, void *dst, const void *src, unsigned long long bytes);
 
 /* Data dumps of the resident state, byte-identical to the reference's:
  * athb_dump_bin writes dump_binary's file (src/dump_binary.c:25-134; the

@@ -25,3 +25,13 @@ def test_neighbours_and_physical_sides():
     assert neighbours(0, 3, False) == (None, 1) and neighbours(2, 3, False) == (1, None)
     assert [x2_sides(r, 3, False) for r in range(3)] == [1, 0, 2]
     assert neighbours(0, 2, True) == (1, 1)
+
+
+def test_transport_is_checked_before_any_device_work():
+    from athena_cuda_b200 import configs
+    from athena_cuda_b200.decomp import MAX_RANKS, SlabGrid
+
+    with pytest.raises(ValueError, match="transport"):
+        SlabGrid(configs.blast(16, 16), "blast", 0, 2, transport="tcp")
+    with pytest.raises(ValueError, match="at most"):
+        SlabGrid(configs.blast(16, 16 * (MAX_RANKS + 1)), "blast", 0, MAX_RANKS + 1, transport="ipc")

@@ -1,7 +1,11 @@
 """A grid split over processes as x2 slabs (athena_cuda_b200/decomp.py) gives
 the single grid's state bit for bit: 2 and 3 ranks, periodic, outflow and
 reflecting x2 boundaries.  The ranks share this one GPU and exchange rows
-through host memory (gloo); no kernel waits on another rank."""
+through host memory (transport "host", gloo) or through device buffers
+(transport "ipc": rows packed on the GPU and copied with cudaMemcpyAsync into
+the neighbours' CUDA-IPC-mapped receive buffers, the 1/dt maximum over device
+words); host barriers order the copies, so no kernel waits on another rank.
+The exchange time per iteration is printed."""
 from __future__ import annotations
 
 import os
@@ -36,7 +40,7 @@ def _free_port() -> int:
         return s.getsockname()[1]
 
 
-def _rank(rank, ranks, port, name, q):
+def _rank(rank, ranks, port, name, transport, q):
     import datetime
 
     import torch.distributed as dist
@@ -48,29 +52,32 @@ def _rank(rank, ranks, port, name, q):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=ranks, timeout=datetime.timedelta(seconds=120))
     try:
-        s = SlabGrid(_blocks(problem, kw), problem, rank, ranks)
+        s = SlabGrid(_blocks(problem, kw), problem, rank, ranks, transport=transport)
         s.run(steps)
+        per_iter_ms = 1e3 * s.exchange_s / max(1, s.iterations)
         full = s.gather()
         st = s.status()
         s.close()
         if rank == 0:
-            q.put((full, st["dt"], st["time"], st["nstep"]))
+            q.put((full, st["dt"], st["time"], st["nstep"], per_iter_ms))
     finally:
         dist.destroy_process_group()
 
 
+@pytest.mark.parametrize("transport", ["host", "ipc"])
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_slabs_equal_single_grid(name):
+def test_slabs_equal_single_grid(name, transport):
     from athena_cuda_b200 import Grid, Params
 
     problem, kw, ranks, steps = CASES[name]
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank, args=(r, ranks, port, name, q)) for r in range(ranks)]
+    procs = [ctx.Process(target=_rank, args=(r, ranks, port, name, transport, q)) for r in range(ranks)]
     for p in procs:
         p.start()
-    full, dt, t, n = q.get(timeout=300)
+    full, dt, t, n, per_iter_ms = q.get(timeout=300)
+    print(f"{name} {transport}: exchange + maximum {per_iter_ms:.3f} ms per iteration")
     for p in procs:
         p.join(timeout=120)
         assert p.exitcode == 0
