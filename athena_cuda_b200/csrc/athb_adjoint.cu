@@ -35,8 +35,27 @@ constexpr int kItemThreads = 128;
 constexpr int kRedThreads = 256;
 constexpr int kRedBlocks = 296;   // 2 per SM of a B200
 
+// Resident 128-thread blocks per SM each stage kernel is compiled for (the
+// register cap = 65536 / (128 x blocks)); 1 leaves the compiler its choice.
+#ifndef ATHB_ADJ_MINB_PLM
+#define ATHB_ADJ_MINB_PLM 1
+#endif
+#ifndef ATHB_ADJ_MINB_RIE
+#define ATHB_ADJ_MINB_RIE 1
+#endif
+#ifndef ATHB_ADJ_MINB_COR
+#define ATHB_ADJ_MINB_COR 1
+#endif
+template <class F> struct ItemMinBlocks { static constexpr int value = 1; };
+template <int STAGE, int FLUX> struct ItemMinBlocks<AdjFn<STAGE, FLUX>> {
+  static constexpr int value = (STAGE == R_PLMX || STAGE == R_PLMY)   ? ATHB_ADJ_MINB_PLM
+                               : (STAGE == R_RIEX || STAGE == R_RIEY) ? ATHB_ADJ_MINB_RIE
+                               : (STAGE == R_CORX || STAGE == R_CORY) ? ATHB_ADJ_MINB_COR
+                                                                      : 1;
+};
+
 template <class F>
-__global__ void __launch_bounds__(kItemThreads) k_items(GenRange r, long long n, F f) {
+__global__ void __launch_bounds__(kItemThreads, ItemMinBlocks<F>::value) k_items(GenRange r, long long n, F f) {
   const long long t = (long long)blockIdx.x * kItemThreads + threadIdx.x;
   if (t >= n) return;
   int j, i;

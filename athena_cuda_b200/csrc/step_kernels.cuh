@@ -231,8 +231,14 @@ __device__ __forceinline__ void predict_y(const GridArgs& g, const PredictGeom& 
 // Resident blocks per SM the heavy kernels are compiled for (register caps of
 // 168 and 128 per thread): measured faster on B200 than the uncapped 255
 // registers and 2 blocks per SM despite the spills they cause.
-constexpr int kPredictMinBlocks = 3;
-constexpr int kCorrectMinBlocks = 4;
+#ifndef ATHB_PREDICT_MIN_BLOCKS
+#define ATHB_PREDICT_MIN_BLOCKS 3
+#endif
+#ifndef ATHB_CORRECT_MIN_BLOCKS
+#define ATHB_CORRECT_MIN_BLOCKS 4
+#endif
+constexpr int kPredictMinBlocks = ATHB_PREDICT_MIN_BLOCKS;
+constexpr int kCorrectMinBlocks = ATHB_CORRECT_MIN_BLOCKS;
 
 // Block b of the predictor: the long role-Y column marches (ly rows each)
 // come first and the short role-X row segments (31 faces) last, so the

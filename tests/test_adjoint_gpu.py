@@ -134,10 +134,17 @@ def test_field_loop_256_dot_product(tmp_path):
     g.close()
 
 
+SWEEP_DIRS, SWEEP_EPS = (2, 6, 7, 10), (1e-4, 1e-5, 1e-7)
+
+
 @pytest.mark.slow
 def test_field_loop_256_finite_differences_of_reference(tmp_path):
     """Central differences of the reference CPU path (32 runs of 200 steps,
-    in parallel) along 16 seeded smooth density directions."""
+    in parallel) along 16 seeded smooth density directions, and for four of
+    them at eps = 1e-4, 1e-5, 1e-7 as well: the map is only piecewise smooth
+    and its evaluation carries ~1e-12 relative rounding, so the differences
+    scatter with eps at the 1e-3 .. 1e-2 level and have no plateau to
+    converge to; the adjoint must lie within that scatter."""
     if not refutil.have_ref("file", "roe"):
         pytest.skip("oracle/_ref not built")
     ath, base, rho = _field_loop_case(tmp_path)
@@ -149,31 +156,38 @@ def test_field_loop_256_finite_differences_of_reference(tmp_path):
     grho = fl.density_gradient(base, grad)
     eps = 1e-6
     dirs = [fl.smoothed_density(NX, NX, 1000 + k, amp=1.0) - 1.0 for k in range(16)]
+    runs = [(k, eps) for k in range(16)] + [(k, e) for k in SWEEP_DIRS for e in SWEEP_EPS]
     procs = []
-    for k, drho in enumerate(dirs):
+    for k, e in runs:
         for s, tag in ((1.0, "p"), (-1.0, "m")):
-            init = refutil.write_raw(tmp_path / f"init_{k}{tag}.bin", fl.density_state(base, rho + s * eps * drho))
-            out = tmp_path / f"out_{k}{tag}.bin"
+            init = refutil.write_raw(tmp_path / f"init_{k}_{e}{tag}.bin", fl.density_state(base, rho + s * e * dirs[k]))
+            out = tmp_path / f"out_{k}_{e}{tag}.bin"
             cmd = [str(refutil.ref_binary("file", "roe")), "-i", str(ath), "--init", str(init), "--dump", str(out)]
-            procs.append((k, tag, out, subprocess.Popen(cmd, cwd=tmp_path, stdout=subprocess.DEVNULL,
-                                                         stderr=subprocess.PIPE)))
+            procs.append((k, e, tag, out, subprocess.Popen(cmd, cwd=tmp_path, stdout=subprocess.DEVNULL,
+                                                            stderr=subprocess.PIPE)))
     Jv = {}
-    for k, tag, out, p in procs:
+    for k, e, tag, out, p in procs:
         _, err = p.communicate(timeout=1800)
         assert p.returncode == 0, err.decode()[-1000:]
         r = refutil.read_raw(out)
         assert r["nstep"] == NSTEPS
-        Jv[(k, tag)] = fl.objective(r["planes"])
-    rows = []
-    for k, drho in enumerate(dirs):
-        fd = (Jv[(k, "p")] - Jv[(k, "m")]) / (2 * eps)
-        ad = float(np.sum(grho * drho))
-        rows.append((k, fd, ad, abs(fd - ad) / abs(ad)))
-    report = "\n".join(f"direction {k:2d}: fd {fd:+.12e} adjoint {ad:+.12e} rel {e:.2e}" for k, fd, ad, e in rows)
+        Jv[(k, e, tag)] = fl.objective(r["planes"])
+    fd = {(k, e): (Jv[(k, e, "p")] - Jv[(k, e, "m")]) / (2 * e) for k, e in runs}
+    ad = [float(np.sum(grho * d)) for d in dirs]
+    rows = [(k, fd[(k, eps)], ad[k], abs(fd[(k, eps)] - ad[k]) / abs(ad[k])) for k in range(16)]
+    report = "\n".join(f"direction {k:2d}: fd {f:+.12e} adjoint {a:+.12e} rel {r:.2e}" for k, f, a, r in rows)
+    sweep = []
+    for k in SWEEP_DIRS:
+        vals = [fd[(k, e)] for e in sorted(SWEEP_EPS + (eps,), reverse=True)]
+        sweep.append(f"direction {k:2d}: eps 1e-4 1e-5 1e-6 1e-7 -> " + " ".join(f"{v:+.6e}" for v in vals)
+                     + f"  adjoint {ad[k]:+.6e}")
+        med = float(np.median(vals))
+        assert abs(ad[k] - med) <= max(abs(v - med) for v in vals) + 1e-3 * abs(med), sweep[-1]
+    report += "\n" + "\n".join(sweep)
     print(report)
     out = Path("gpurun_out") if Path("gpurun_out").is_dir() else Path(tempfile.gettempdir())
     (out / "athb_fd_report.txt").write_text(report + "\n")
-    assert sorted(e for _, _, _, e in rows)[len(rows) // 2] <= 1e-2, report
+    assert sorted(r for _, _, _, r in rows)[len(rows) // 2] <= 1e-2, report
 
 
 def test_torch_autograd_function(tmp_path):
