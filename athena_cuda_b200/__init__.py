@@ -127,6 +127,7 @@ def lib() -> C.CDLL:
             "athb_get_ly": (I, [P]),
             "athb_host_free": (None, [P]),
             "athb_tlm_run": (I, [P, I, dp, dp, dp, dp]),
+            "athb_adjoint_keep_workspace": (I, [P, I]),
             "athb_adjoint_gradient": (I, [P, I, C.c_longlong, dp, dp, C.POINTER(AdjointStats)]),
         }
         for name, (res, args) in sig.items():
@@ -313,6 +314,11 @@ class Grid:
         _check(lib().athb_tlm_run(self._h, nsteps, _dp(d), C.byref(J), C.byref(dJ),
                                   _dp(out) if out is not None else None))
         return (J.value, dJ.value, out) if want_state else (J.value, dJ.value)
+
+    def keep_adjoint_workspace(self, on: bool = True) -> None:
+        """Keep the adjoint's device workspace between calls (a repeated
+        gradient of the same size allocates nothing), or free it now."""
+        _check(lib().athb_adjoint_keep_workspace(self._h, int(on)))
 
     def adjoint_gradient(self, nsteps: int, snapshot_bytes: int = 0):
         """Adjoint of nsteps main-loop iterations from the resident state:

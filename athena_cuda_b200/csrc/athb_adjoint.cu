@@ -170,13 +170,46 @@ struct SetStFn {
   }
 };
 
+}  // namespace
+
+// Device blocks kept between adjoint calls: (pointer, bytes), unused by the
+// call in flight.
+struct athb_adj_cache {
+  std::vector<std::pair<void*, size_t>> blocks;
+};
+
+namespace {
+
+void* cache_take(athb_adj_cache* c, size_t b) {
+  for (auto it = c->blocks.begin(); it != c->blocks.end(); ++it)
+    if (it->second == b) {
+      void* p = it->first;
+      c->blocks.erase(it);
+      return p;
+    }
+  return nullptr;
+}
+void cache_put(athb_adj_cache* c, void* p, size_t b) { c->blocks.emplace_back(p, b); }
+// free every cached block; true if there were any
+bool cache_drop_all(athb_adj_cache* c) {
+  const bool any = !c->blocks.empty();
+  for (auto& bl : c->blocks) cudaFree(bl.first);
+  c->blocks.clear();
+  return any;
+}
+size_t cache_bytes(const athb_adj_cache* c) {
+  size_t n = 0;
+  for (auto& bl : c->blocks) n += bl.second;
+  return n;
+}
+
 struct GpuExec {
   cudaStream_t s = nullptr;
   StepState* st = nullptr;     // StepState of the fast kernels
   cudaError_t err = cudaSuccess;
   double* red = nullptr;       // reduction partials
   MaxLoc* redm = nullptr;
-  std::vector<void*> owned;
+  std::vector<std::pair<void*, size_t>> owned;
   size_t bytes = 0;
 
   void note(cudaError_t e) { if (e != cudaSuccess && err == cudaSuccess) err = e; }
@@ -254,20 +287,36 @@ struct GpuExec {
     d.cfl(d.pd(d.S[cur ^ 1]), d.pd(d.tape + (size_t)G_DTI * G.ps));
   }
 
+  // With a cache (athb_adjoint_keep_workspace on) a block of the same size
+  // left by the previous call is reused, released blocks go back to the
+  // cache, and a failed cudaMalloc first gives the unused cached blocks back.
+  athb_adj_cache* cache = nullptr;
   void* alloc_bytes(size_t b) {
     void* p = nullptr;
     if (err != cudaSuccess) return nullptr;
-    cudaError_t e = cudaMalloc(&p, b ? b : 8);
+    b = b ? b : 8;
+    if (cache && (p = cache_take(cache, b)) != nullptr) {
+      owned.emplace_back(p, b);
+      bytes += b;
+      return p;
+    }
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e == cudaErrorMemoryAllocation && cache && cache_drop_all(cache)) {
+      (void)cudaGetLastError();
+      e = cudaMalloc(&p, b);
+    }
     note(e);
-    if (e == cudaSuccess) { owned.push_back(p); bytes += b; }
+    if (e == cudaSuccess) { owned.emplace_back(p, b); bytes += b; }
     return e == cudaSuccess ? p : nullptr;
   }
   double* alloc(size_t n) { return (double*)alloc_bytes(n * sizeof(double)); }
   void release_bytes(void* p) {
     if (!p) return;
-    auto it = std::find(owned.begin(), owned.end(), p);
-    if (it != owned.end()) owned.erase(it);
-    cudaFree(p);
+    size_t b = 0;
+    for (auto it = owned.begin(); it != owned.end(); ++it)
+      if (it->first == p) { b = it->second; owned.erase(it); break; }
+    if (cache && b) cache_put(cache, p, b);
+    else cudaFree(p);
   }
   void release(double* p) { release_bytes(p); }
   void zero(double* p, size_t n) { if (err == cudaSuccess) note(cudaMemsetAsync(p, 0, n * sizeof(double), s)); }
@@ -281,7 +330,10 @@ struct GpuExec {
     note(cudaStreamSynchronize(s));
   }
   ~GpuExec() {
-    for (void* p : owned) cudaFree(p);
+    for (auto& o : owned) {
+      if (cache) cache_put(cache, o.first, o.second);
+      else cudaFree(o.first);
+    }
   }
 };
 
@@ -340,6 +392,7 @@ extern "C" int athb_tlm_run(athb_ctx* ctx, int nsteps, const double* dstate0, do
   CUDA_TRY(cudaSetDevice(ctx->cfg.device));
   GpuExec x;
   x.s = ctx->stream;
+  x.cache = ctx->adj_keep ? ctx->adj_cache : nullptr;
   AdjointDriver<GpuExec> d(x, geom_of(ctx));
   x.red = x.alloc(kRedBlocks);
   x.redm = (MaxLoc*)x.alloc_bytes(sizeof(MaxLoc) * kRedBlocks);
@@ -372,6 +425,7 @@ extern "C" int athb_adjoint_gradient(athb_ctx* ctx, int nsteps, long long snapsh
   const auto t0 = std::chrono::steady_clock::now();
   GpuExec x;
   x.s = ctx->stream;
+  x.cache = ctx->adj_keep ? ctx->adj_cache : nullptr;
   AdjointDriver<GpuExec> d(x, geom_of(ctx));
   x.red = x.alloc(kRedBlocks);
   x.redm = (MaxLoc*)x.alloc_bytes(sizeof(MaxLoc) * kRedBlocks);
@@ -383,6 +437,7 @@ extern "C" int athb_adjoint_gradient(athb_ctx* ctx, int nsteps, long long snapsh
   if (budget <= 0) {
     size_t fr = 0, tot = 0;
     CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+    if (x.cache) fr += cache_bytes(x.cache);   // kept blocks are this call's to reuse
     budget = (long long)(0.85 * (double)fr) - (1LL << 30);   // keep 1 GiB of headroom
   }
   const size_t tbytes = sizeof(double) * d.tape_doubles();
@@ -416,4 +471,28 @@ extern "C" int athb_adjoint_gradient(athb_ctx* ctx, int nsteps, long long snapsh
     stats->tape_mode = d.tapes != nullptr;
   }
   return ATHB_OK;
+}
+
+// Keep (on != 0) the adjoint's device workspace between calls on this
+// context, or free it now (on == 0).
+extern "C" int athb_adjoint_keep_workspace(athb_ctx* ctx, int on) {
+  if (!ctx) return athb_fail(ATHB_ERR_ARG, "null context");
+  CUDA_TRY(cudaSetDevice(ctx->cfg.device));
+  if (on) {
+    if (!ctx->adj_cache) ctx->adj_cache = new athb_adj_cache;
+    ctx->adj_keep = 1;
+  } else {
+    athb_adjoint_cache_free(ctx);
+  }
+  return ATHB_OK;
+}
+
+void athb_adjoint_cache_free(athb_ctx* c) {
+  if (!c || !c->adj_cache) return;
+  cudaSetDevice(c->cfg.device);
+  cudaStreamSynchronize(c->stream);
+  cache_drop_all(c->adj_cache);
+  delete c->adj_cache;
+  c->adj_cache = nullptr;
+  c->adj_keep = 0;
 }

@@ -163,6 +163,7 @@ extern "C" void athb_destroy(athb_ctx* c) {
   cudaFree(c->st);
   cudaFree(c->aos);
   cudaFree(c->cpaw_soln);
+  athb_adjoint_cache_free(c);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }

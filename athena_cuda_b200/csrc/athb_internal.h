@@ -29,7 +29,12 @@ struct athb_ctx {
   // cpaw2d reference solution: planes d .. B3c of the initial state, kept on
   // the device in the state layout (stride ps, row pitch)
   double* cpaw_soln = nullptr;
+  // device blocks of the last adjoint / tangent-linear call, kept for the
+  // next call when athb_adjoint_keep_workspace is on (athb_adjoint.cu)
+  struct athb_adj_cache* adj_cache = nullptr;
+  int adj_keep = 0;
 };
+void athb_adjoint_cache_free(athb_ctx* c);
 
 // internal helpers (athb_core.cu)
 int athb_fail(int code, const char* fmt, ...);

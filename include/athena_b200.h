@@ -386,6 +386,12 @@ int athb_tlm_run(athb_ctx *ctx, int nsteps, const double *dstate0, double *J, do
  * 1992) recomputes the fewest forward steps the room allows.                */
 int athb_adjoint_gradient(athb_ctx *ctx, int nsteps, long long snapshot_bytes, double *J, double *grad,
                           athb_adjoint_stats *stats);
+/* Keep the device workspace of athb_adjoint_gradient / athb_tlm_run on this
+ * context between calls (on = 1: a repeated call of the same size reuses it
+ * instead of allocating and freeing up to most of the GPU's memory; the
+ * default budget counts the kept blocks as free), or free it now (on = 0,
+ * the default state).  athb_destroy frees it too.  No reference counterpart. */
+int athb_adjoint_keep_workspace(athb_ctx *ctx, int on);
 
 /* ---- allocation-free step ------------------------------------------------ */
 /* No counterpart in the reference.  One integrate_2d step (the cells

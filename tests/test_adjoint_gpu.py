@@ -220,3 +220,25 @@ def test_torch_autograd_function(tmp_path):
     _, dJ = g.tlm(n, fl.density_direction(base, drho))
     assert abs(float(torch.sum(rho.grad * torch.from_numpy(drho))) - 2.0 * dJ) <= 1e-10 * abs(2.0 * dJ)
     g.close()
+
+
+def test_kept_workspace_gives_the_same_gradient(tmp_path):
+    """athb_adjoint_keep_workspace: repeated calls reuse the kept blocks and
+    give the same gradient bit for bit, in tape mode and with binomial
+    checkpointing; switching it off frees them."""
+    blocks = configs.blast(40, 32)
+    g = Grid.from_athinput(write_athinput(tmp_path / "athinput", blocks), "blast")
+    J0, g0, _ = g.adjoint_gradient(12)
+    g.keep_adjoint_workspace(True)
+    pitch = (40 + 8 + 15) // 16 * 16
+    state_bytes = 11 * 8 * pitch * (32 + 8)
+    for snap in (0, 0, 4 * state_bytes, 4 * state_bytes, 0):
+        J, g1, st = g.adjoint_gradient(12, snapshot_bytes=snap)
+        assert J == J0 and np.array_equal(g1, g0), snap
+    _, dJ0 = g.tlm(12, np.ones_like(g0))
+    _, dJ1 = g.tlm(12, np.ones_like(g0))
+    assert dJ0 == dJ1
+    g.keep_adjoint_workspace(False)
+    J, g1, _ = g.adjoint_gradient(12)
+    assert J == J0 and np.array_equal(g1, g0)
+    g.close()
