@@ -278,25 +278,6 @@ ATHB_HD void prim_add_arr(Prim1& w, const double a[7]) {
 // --- src/lr_states_plm.c:95-233, one cell -------------------------------------
 // Forward: plm_cell(wm, w0, wp, bxc, dtodx) -> (wl_next, wr_this).
 // Adjoint: wlb, wrb (adjoints of wl_next, wr_this) -> wmb, w0b, wpb, bxcb, dtodxb.
-// Steps 2-3 of the PLM (src/lr_states_plm.c:106-133): centred, left, right
-// and van Leer differences and their characteristic projections.
-ATHB_HD void plm_slopes(const PrimEig& E, const double Wm[7], const double W0[7], const double Wp[7],
-                        double dWc[7], double dWl[7], double dWr[7], double dWg[7], double dac[7], double dal[7],
-                        double dar[7], double dag[7]) {
-  #pragma unroll
-  for (int n = 0; n < 7; n++) {
-    dWc[n] = Wp[n] - Wm[n];
-    dWl[n] = W0[n] - Wm[n];
-    dWr[n] = Wp[n] - W0[n];
-    if (dWl[n] * dWr[n] > 0.0) dWg[n] = 2.0 * dWl[n] * dWr[n] / (dWl[n] + dWr[n]);
-    else dWg[n] = 0.0;
-  }
-  prim_project(E, dWc, dac);
-  prim_project(E, dWl, dal);
-  prim_project(E, dWr, dar);
-  prim_project(E, dWg, dag);
-}
-
 ATHB_HD void plm_cell_adj(const Prim1& wm, const Prim1& w0, const Prim1& wp, double bxc, double dtodx,
                           const Eos& eos, const Prim1& wlb, const Prim1& wrb, Prim1& wmb, Prim1& w0b, Prim1& wpb,
                           double& bxcb, double& dtodxb) {
@@ -305,21 +286,28 @@ ATHB_HD void plm_cell_adj(const Prim1& wm, const Prim1& w0, const Prim1& wp, dou
   esys_prim(w0.d, w0.vx, w0.p, bxc, w0.by, w0.bz, eos, E);
   double Wm[7], W0[7], Wp[7];
   prim_arr(wm, Wm); prim_arr(w0, W0); prim_arr(wp, Wp);
-  // the slopes and projections are not kept: the reverse of step 4
-  // recomputes them (the same operations, so the same values), which keeps
-  // 56 doubles out of the live set across the reverse of steps 9-5
+  double dWc[7], dWl[7], dWr[7], dWg[7];
+  #pragma unroll
+  for (int n = 0; n < 7; n++) {
+    dWc[n] = Wp[n] - Wm[n];
+    dWl[n] = W0[n] - Wm[n];
+    dWr[n] = Wp[n] - W0[n];
+    if (dWl[n] * dWr[n] > 0.0) dWg[n] = 2.0 * dWl[n] * dWr[n] / (dWl[n] + dWr[n]);
+    else dWg[n] = 0.0;
+  }
+  double dac[7], dal[7], dar[7], dag[7];
+  prim_project(E, dWc, dac);
+  prim_project(E, dWl, dal);
+  prim_project(E, dWr, dar);
+  prim_project(E, dWg, dag);
   double da[7];
-  {
-    double dWc[7], dWl[7], dWr[7], dWg[7], dac[7], dal[7], dar[7], dag[7];
-    plm_slopes(E, Wm, W0, Wp, dWc, dWl, dWr, dWg, dac, dal, dar, dag);
-    #pragma unroll
-    for (int n = 0; n < 7; n++) {
-      da[n] = 0.0;
-      if (dal[n] * dar[n] > 0.0) {
-        const double lim_slope1 = rmin(fabs(dal[n]), fabs(dar[n]));
-        const double lim_slope2 = rmin(0.5 * fabs(dac[n]), fabs(dag[n]));
-        da[n] = rsign(dac[n]) * rmin(2.0 * lim_slope1, lim_slope2);
-      }
+  #pragma unroll
+  for (int n = 0; n < 7; n++) {
+    da[n] = 0.0;
+    if (dal[n] * dar[n] > 0.0) {
+      const double lim_slope1 = rmin(fabs(dal[n]), fabs(dar[n]));
+      const double lim_slope2 = rmin(0.5 * fabs(dac[n]), fabs(dag[n]));
+      da[n] = rsign(dac[n]) * rmin(2.0 * lim_slope1, lim_slope2);
     }
   }
   double dWm[7];
@@ -498,9 +486,7 @@ ATHB_HD void plm_cell_adj(const Prim1& wm, const Prim1& w0, const Prim1& wp, dou
   Eb.R40 += dWmb[4] * (da[0] + da[6]); Eb.R42 += dWmb[4] * (da[2] + da[4]);
   Eb.R50 += dWmb[5] * (da[0] + da[6]); Eb.R51 += dWmb[5] * (da[1] + da[5]); Eb.R52 += dWmb[5] * (da[2] + da[4]);
   Eb.R60 += dWmb[6] * (da[0] + da[6]); Eb.R61 += dWmb[6] * (da[1] + da[5]); Eb.R62 += dWmb[6] * (da[2] + da[4]);
-  // step 4: limiter, branch frozen (slopes and projections recomputed)
-  double dWc[7], dWl[7], dWr[7], dWg[7], dac[7], dal[7], dar[7], dag[7];
-  plm_slopes(E, Wm, W0, Wp, dWc, dWl, dWr, dWg, dac, dal, dar, dag);
+  // step 4: limiter, branch frozen
   double dacb[7] = {0, 0, 0, 0, 0, 0, 0}, dalb[7] = {0, 0, 0, 0, 0, 0, 0};
   double darb[7] = {0, 0, 0, 0, 0, 0, 0}, dagb[7] = {0, 0, 0, 0, 0, 0, 0};
   #pragma unroll
@@ -1111,20 +1097,6 @@ ATHB_HD void flux_hlle_adj(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, co
 }
 
 // --- src/flux_roe.c:54-259 -----------------------------------------------------
-// The HLLE fallback of the Roe adjoint, out of line on the device: it runs
-// only where the forward fell back, and inlined it would set the register
-// budget of every Roe face.
-#ifdef __CUDACC__
-__host__ __device__ __noinline__
-#else
-static
-#endif
-void flux_hlle_adj_outlined(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const Prim1& Wr, double Bxi,
-                            const Eos& eos, const Cons1& Fb, Cons1& Ulb, Cons1& Urb, Prim1& Wlb, Prim1& Wrb,
-                            double& Bxib) {
-  flux_hlle_adj(Ul, Ur, Wl, Wr, Bxi, eos, Fb, Ulb, Urb, Wlb, Wrb, Bxib);
-}
-
 ATHB_HD void flux_roe_adj(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, const Prim1& Wr, double Bxi,
                           const Eos& eos, const Cons1& Fb, Cons1& Ulb, Cons1& Urb, Prim1& Wlb, Prim1& Wrb,
                           double& Bxib) {
@@ -1168,7 +1140,7 @@ ATHB_HD void flux_roe_adj(const Cons1& Ul, const Cons1& Ur, const Prim1& Wl, con
           bad = (p_inter < 0.0);
         }
         if (bad) {
-          flux_hlle_adj_outlined(Ul, Ur, Wl, Wr, Bxi, eos, Fb, Ulb, Urb, Wlb, Wrb, Bxib);
+          flux_hlle_adj(Ul, Ur, Wl, Wr, Bxi, eos, Fb, Ulb, Urb, Wlb, Wrb, Bxib);
           return;
         }
       }
