@@ -107,6 +107,8 @@ def lib() -> C.CDLL:
             "athb_batch_set_ly": (I, [P, I, I]),
             "athb_batch_commit": (I, [P]),
             "athb_batch_set_grid": (I, [P, I]),
+            "athb_batch_set_threads": (I, [P, I]),
+            "athb_batch_threads": (I, [P]),
             "athb_batch_grid": (I, [P]),
             "athb_batch_timing": (I, [P, I, dp]),
             "athb_batch_set_mode": (I, [P, I]),
@@ -483,6 +485,16 @@ class Batch:
     @property
     def grid(self) -> int:
         return lib().athb_batch_grid(self._h)
+
+    @property
+    def threads(self) -> int:
+        """Threads per work unit of the phased launches (64, 128, 256)."""
+        return lib().athb_batch_threads(self._h)
+
+    @threads.setter
+    def threads(self, nt: int) -> None:
+        _check(lib().athb_batch_set_threads(self._h, nt))
+        self.commit()
 
     PERSISTENT, PHASED = 0, 1
 

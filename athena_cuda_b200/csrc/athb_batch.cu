@@ -44,6 +44,8 @@ struct InstGeom {
   PredictGeom pg;
   CorrectGeom cg;
   int nx1, nx2, sx, sy, nframe;
+  int nt;      // threads per work unit (the block size of the phase launches)
+  int pad;
 };
 
 struct BarrierState {
@@ -93,7 +95,8 @@ __device__ __forceinline__ unsigned long long global_ns() {
 
 // Units of instance I in map segment seg.
 __host__ __device__ inline int item_count(const InstGeom& I, int seg) {
-  auto bf = [](long long n) { return (int)((n + kThreads - 1) / kThreads); };
+  const int nt = I.nt;
+  auto bf = [nt](long long n) { return (int)((n + nt - 1) / nt); };
   switch (seg) {
   case kSegPredictY: return I.pg.ny_blocks;
   case kSegPredictX: return I.pg.nx_blocks;
@@ -143,7 +146,7 @@ __global__ void k_barrier_selftest(BarrierState* bar, int* err, long long spins)
 __device__ __forceinline__ void load_geom(const BatchDev& B, InstGeom& s_I, int k, int cur) {
   constexpr int kWords = (int)(sizeof(InstGeom) / sizeof(unsigned long long));
   static_assert(sizeof(InstGeom) % sizeof(unsigned long long) == 0, "InstGeom copy granularity");
-  static_assert(kWords <= kThreads, "InstGeom copy width");
+  static_assert(kWords <= 64, "InstGeom copy width (the smallest block has 64 threads)");
   if (threadIdx.x < kWords)
     reinterpret_cast<unsigned long long*>(&s_I)[threadIdx.x] =
         reinterpret_cast<const unsigned long long*>(&B.inst[k])[threadIdx.x];
@@ -156,24 +159,25 @@ __device__ __forceinline__ void load_geom(const BatchDev& B, InstGeom& s_I, int 
   __syncthreads();
 }
 
-// Units b0 .. b0+nb-1 of phase ph of instance k (geometry I).
-template <int FLUX>
+// Units b0 .. b0+nb-1 of phase ph of instance k (geometry I), NT threads
+// per unit (the block size).
+template <int FLUX, int NT>
 __device__ __forceinline__ void run_chunk(const BatchDev& B, int ph, int k, int b0, int nb, const InstGeom& I) {
   const GridArgs& g = I.g;
   switch (ph) {
   case 0:
-    for (int u = 0; u < nb; u++) predict_block<FLUX>(g, I.pg, b0 + u);
+    for (int u = 0; u < nb; u++) predict_block<FLUX, false, NT>(g, I.pg, b0 + u);
     break;
   case 1:
     for (int u = 0; u < nb; u++)
-      emf_item(g, g.is - 1, g.js - 1, I.nx1 + 3, I.nx2 + 3, S_FX, S_FY, (b0 + u) * kThreads + threadIdx.x);
+      emf_item(g, g.is - 1, g.js - 1, I.nx1 + 3, I.nx2 + 3, S_FX, S_FY, (b0 + u) * NT + threadIdx.x);
     break;
   case 2:
-    for (int u = 0; u < nb; u++) correct_block<FLUX>(g, I.cg, b0 + u);
+    for (int u = 0; u < nb; u++) correct_block<FLUX, NT>(g, I.cg, b0 + u);
     break;
   case 3:
     for (int u = 0; u < nb; u++)
-      emf_item(g, g.is, g.js, I.nx1 + 1, I.nx2 + 1, S_FX2, S_FY2, (b0 + u) * kThreads + threadIdx.x);
+      emf_item(g, g.is, g.js, I.nx1 + 1, I.nx2 + 1, S_FX2, S_FY2, (b0 + u) * NT + threadIdx.x);
     break;
   case 4: {
     // the CFL rate max over the chunk, then one block reduction (max is
@@ -181,16 +185,16 @@ __device__ __forceinline__ void run_chunk(const BatchDev& B, int ph, int k, int 
     double m = 0.0;
     bool bad = false;
     for (int u = 0; u < nb; u++) {
-      const double v = update_cell(g, I.nx1, I.nx1 * I.nx2, (b0 + u) * kThreads + threadIdx.x);
+      const double v = update_cell(g, I.nx1, I.nx1 * I.nx2, (b0 + u) * NT + threadIdx.x);
       if (!(v >= 0.0) || isinf(v)) bad = true;
       else m = fmax(m, v);
     }
     if (bad) atomicOr(&g.st->flags, kErrNonFinite);
-    block_max_to(m, &g.st->max_dti_bits, &g.st->flags);
+    block_max_to<NT>(m, &g.st->max_dti_bits, &g.st->flags);
     break;
   }
   default: {
-    for (int u = 0; u < nb; u++) ghost_item(g, I.sx, I.sy, I.nframe, 3, 3, (b0 + u) * kThreads + threadIdx.x);
+    for (int u = 0; u < nb; u++) ghost_item(g, I.sx, I.sy, I.nframe, 3, 3, (b0 + u) * NT + threadIdx.x);
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();
@@ -253,7 +257,7 @@ __global__ void __launch_bounds__(kThreads, kBatchMinBlocks) k_batch_step(BatchD
           k_prev = s_k;
           cur_prev = s_load - 1;
         }
-        run_chunk<FLUX>(B, ph, s_k, s_b, s_nb, s_I);
+        run_chunk<FLUX, kThreads>(B, ph, s_k, s_b, s_nb, s_I);
       }
       if (threadIdx.x == 0) s_w = (int)nxt;
       __syncthreads();  // S2: the item is finished with s_I; the next ticket is visible
@@ -271,13 +275,16 @@ __global__ void __launch_bounds__(kThreads, kBatchMinBlocks) k_batch_step(BatchD
 // Phased execution: one launch per phase, one work item per block (the
 // hardware block scheduler balances), each phase with the register budget of
 // its single-grid kernel.
-template <int PH>
+// The register budget per thread stays that of the 128-thread single-grid
+// kernels where the block size allows it (64 threads: twice the blocks).
+template <int PH, int NT>
 struct PhaseBlocks {
-  static constexpr int value = PH == 0 ? kPredictMinBlocks : PH == 2 ? kCorrectMinBlocks : 1;
+  static constexpr int at128 = PH == 0 ? kPredictMinBlocks : PH == 2 ? kCorrectMinBlocks : 1;
+  static constexpr int value = at128 * kThreads / NT > 0 ? at128 * kThreads / NT : 1;
 };
 
-template <int FLUX, int PH>
-__global__ void __launch_bounds__(kThreads, PhaseBlocks<PH>::value) k_batch_phase(BatchDev B) {
+template <int FLUX, int PH, int NT>
+__global__ void __launch_bounds__(NT, (PhaseBlocks<PH, NT>::value)) k_batch_phase(BatchDev B) {
   __shared__ InstGeom s_I;
   __shared__ int s_k, s_b, s_nb, s_cur;
   const int base = B.mbase[seg_first(PH)];
@@ -292,7 +299,7 @@ __global__ void __launch_bounds__(kThreads, PhaseBlocks<PH>::value) k_batch_phas
   __syncthreads();
   if (s_cur < 0) return;  // instance has reached its end time
   load_geom(B, s_I, s_k, s_cur);
-  run_chunk<FLUX>(B, PH, s_k, s_b, s_nb, s_I);
+  run_chunk<FLUX, NT>(B, PH, s_k, s_b, s_nb, s_I);
 }
 
 // Phase timing of the phased mode: the time since the previous stamp, added
@@ -347,6 +354,7 @@ struct athb_batch {
   unsigned long long* timing = nullptr;  // per-phase ns (when enabled), then a stamp
   bool timing_on = false;
   int mode = ATHB_BATCH_PHASED;
+  int nt = kThreads;           // threads per work unit (phased mode: 64, 128 or 256)
   int phase_total[kPhases] = {0, 0, 0, 0, 0, 0};  // work items per phase (active set)
   cudaStream_t stream = nullptr;
   int grid = 0;            // persistent blocks
@@ -368,7 +376,7 @@ static int pick_ly(int nx1, int nx2) {
 }
 
 // Geometry of instance k (same rules as the single-grid launcher).
-static InstGeom make_geom(const athb_config& c, int ly, double* state0, double* state1, double* scr,
+static InstGeom make_geom(const athb_config& c, int ly, int nt, double* state0, double* state1, double* scr,
                           StepState* st) {
   InstGeom I;
   memset(&I, 0, sizeof I);
@@ -384,11 +392,12 @@ static InstGeom make_geom(const athb_config& c, int ly, double* state0, double* 
   g.eos = Eos{c.gamma, c.gamma - 1.0, c.gamma - 2.0};
   g.bc[0] = c.bc_ix1; g.bc[1] = c.bc_ox1; g.bc[2] = c.bc_ix2; g.bc[3] = c.bc_ox2;
   const int nx1 = c.nx1, nx2 = c.nx2;
-  I.pg = make_predict_geom(nx1, nx2, ly);
+  I.nt = nt;
+  I.pg = make_predict_geom(nx1, nx2, ly, nt);
   I.cg.xw = nx1 + 1; I.cg.xn = nx2 + 3;
   I.cg.yw = nx1 + 3; I.cg.yn = nx2 + 1;
   I.cg.ew = nx1 + 3; I.cg.en = nx2 + 3;
-  auto bf = [](long long n) { return (int)((n + kThreads - 1) / kThreads); };
+  auto bf = [nt](long long n) { return (int)((n + nt - 1) / nt); };
   I.cg.xb = bf((long long)I.cg.xw * I.cg.xn);
   I.cg.yb = bf((long long)I.cg.yw * I.cg.yn);
   I.cg.eb = bf((long long)I.cg.ew * I.cg.en);
@@ -536,7 +545,7 @@ extern "C" int athb_batch_create(int n, const athb_config* cfgs, athb_batch** ou
     const int sx = cfgs[k].nx1 + 2 * kNghost, sy = cfgs[k].nx2 + 2 * kNghost;
     const size_t ps = (size_t)((sx + 15) & ~15) * sy;
     double* p = b->pool + base[k];
-    b->geom[k] = make_geom(cfgs[k], b->ly[k], p, p + ps * NSTATE, p + 2 * ps * NSTATE, b->st + k);
+    b->geom[k] = make_geom(cfgs[k], b->ly[k], b->nt, p, p + ps * NSTATE, p + 2 * ps * NSTATE, b->st + k);
   }
   int rc = upload_tables(b);
   if (rc) { release(b); return rc; }
@@ -562,9 +571,24 @@ extern "C" int athb_batch_set_ly(athb_batch* b, int k, int ly) {
   b->ly[k] = ly;
   InstGeom& I = b->geom[k];
   const double* s0 = I.g.in;
-  b->geom[k] = make_geom(b->cfg[k], ly, const_cast<double*>(s0), I.g.out, I.g.scr, I.g.st);
+  b->geom[k] = make_geom(b->cfg[k], ly, b->nt, const_cast<double*>(s0), I.g.out, I.g.scr, I.g.st);
   return ATHB_OK;
 }
+
+// Threads per work unit of the phased launches (64, 128 or 256), applied to
+// every instance by athb_batch_commit.  The persistent kernel keeps 128.
+extern "C" int athb_batch_set_threads(athb_batch* b, int nt) {
+  if (!b || (nt != 64 && nt != 128 && nt != 256)) return athb_fail(ATHB_ERR_ARG, "threads per unit: 64, 128 or 256");
+  if (nt != kThreads && b->mode != ATHB_BATCH_PHASED)
+    return athb_fail(ATHB_ERR_ARG, "the persistent mode runs 128-thread units");
+  b->nt = nt;
+  for (int k = 0; k < b->n; k++) {
+    InstGeom& I = b->geom[k];
+    b->geom[k] = make_geom(b->cfg[k], b->ly[k], nt, const_cast<double*>(I.g.in), I.g.out, I.g.scr, I.g.st);
+  }
+  return ATHB_OK;
+}
+extern "C" int athb_batch_threads(const athb_batch* b) { return b ? b->nt : -1; }
 extern "C" int athb_batch_commit(athb_batch* b) {
   if (!b) return athb_fail(ATHB_ERR_ARG, "null batch");
   return upload_tables(b);
@@ -696,7 +720,20 @@ static BatchDev batch_dev(const athb_batch* b) {
 
 template <int FLUX, int PH>
 static cudaError_t launch_phase(const athb_batch* b, const BatchDev& D) {
-  if (b->phase_total[PH] > 0) k_batch_phase<FLUX, PH><<<b->phase_total[PH], kThreads, 0, b->stream>>>(D);
+  if (b->phase_total[PH] > 0) {
+    if (b->nt == 64) k_batch_phase<FLUX, PH, 64><<<b->phase_total[PH], 64, 0, b->stream>>>(D);
+    else if (b->nt == 256) {
+      // the predictor's role-Y ring in dynamic shared memory (see predict_y)
+      const int smem = PH == 0 ? 4 * 7 * 256 * (int)sizeof(double) : 0;
+      if (smem) {
+        cudaError_t e = cudaFuncSetAttribute(k_batch_phase<FLUX, PH, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             smem);
+        if (e != cudaSuccess) return e;
+      }
+      k_batch_phase<FLUX, PH, 256><<<b->phase_total[PH], 256, smem, b->stream>>>(D);
+    }
+    else k_batch_phase<FLUX, PH, kThreads><<<b->phase_total[PH], kThreads, 0, b->stream>>>(D);
+  }
   if (b->timing_on) k_stamp<<<1, 1, 0, b->stream>>>(b->timing, PH);
   return cudaGetLastError();
 }
@@ -873,6 +910,8 @@ extern "C" int athb_batch_selftest_barrier(int device, long long spins, int* tim
 extern "C" int athb_batch_set_mode(athb_batch* b, int mode) {
   if (!b || (mode != ATHB_BATCH_PERSISTENT && mode != ATHB_BATCH_PHASED))
     return athb_fail(ATHB_ERR_ARG, "bad arguments");
+  if (mode == ATHB_BATCH_PERSISTENT && b->nt != kThreads)
+    return athb_fail(ATHB_ERR_ARG, "the persistent mode runs 128-thread units (athb_batch_set_threads)");
   CUDA_TRY(cudaSetDevice(b->device));
   b->mode = mode;
   drop_graph(b);

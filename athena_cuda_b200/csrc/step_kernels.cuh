@@ -86,7 +86,6 @@ __device__ __forceinline__ Cons1 load_cons(const double* base, long long ps, lon
 
 // Launch geometry shared by the host launcher and the kernels.
 constexpr int kThreads = 128;
-constexpr int kXRowsPerBlock = kThreads / 32;   // role X: one warp per row segment
 constexpr int kXFacesPerWarp = 31;              // 32 PLM cells -> 31 faces
 
 // Role X: a warp per 31-face row segment, four rows per block.  Role Y: one
@@ -98,15 +97,17 @@ struct PredictGeom {
 };
 
 // Faces [is-1, ie+2] x rows [js-2, je+2] (role X) and columns [is-2, ie+2]
-// x faces [js-1, je+2] (role Y) of an nx1 x nx2 interior.
-inline PredictGeom make_predict_geom(int nx1, int nx2, int ly) {
+// x faces [js-1, je+2] (role Y) of an nx1 x nx2 interior, in blocks of nt
+// threads (a multiple of 32; the single-grid kernels use kThreads).
+inline PredictGeom make_predict_geom(int nx1, int nx2, int ly, int nt = kThreads) {
   PredictGeom pg;
+  const int rows_per_block = nt / 32;
   pg.xseg = (nx1 + 3 + kXFacesPerWarp - 1) / kXFacesPerWarp;
-  pg.xrowblk = (nx2 + 4 + kXRowsPerBlock - 1) / kXRowsPerBlock;
+  pg.xrowblk = (nx2 + 4 + rows_per_block - 1) / rows_per_block;
   pg.nx_blocks = pg.xseg * pg.xrowblk;
   pg.ycols = nx1 + 4;
   pg.yseg = (nx2 + 3 + ly - 1) / ly;
-  pg.ny_blocks = (int)(((long long)pg.ycols * pg.yseg + kThreads - 1) / kThreads);
+  pg.ny_blocks = (int)(((long long)pg.ycols * pg.yseg + nt - 1) / nt);
   return pg;
 }
 
@@ -120,11 +121,11 @@ __device__ __forceinline__ void store_prim(double* base, long long ps, long long
   base[4 * ps + o] = w.p; base[5 * ps + o] = w.by; base[6 * ps + o] = w.bz;
 }
 
-template <int FLUX, bool TAPE = false>
+template <int FLUX, bool TAPE = false, int NT = kThreads>
 __device__ __forceinline__ void predict_x(const GridArgs& g, int bx, int by) {
   const StepState& st = *g.st;
   const int lane = threadIdx.x & 31;
-  const int j = g.js - 2 + by * kXRowsPerBlock + (threadIdx.x >> 5);
+  const int j = g.js - 2 + by * (NT / 32) + (threadIdx.x >> 5);
   if (j > g.je + 2) return;                        // warp-uniform
   const int c = g.is - 2 + bx * kXFacesPerWarp + lane;
   const int ce = c < g.ie + 3 ? c : g.ie + 3;      // keep c+1 inside the array
@@ -169,41 +170,52 @@ __device__ __forceinline__ void predict_x(const GridArgs& g, int bx, int by) {
 
 // The y role carries three cell states and one face state from row to row;
 // they live in a per-thread ring in shared memory rather than in registers.
+template <int NT = kThreads>
 __device__ __forceinline__ void sh_store(double* sh, int slot, int tid, const Prim1& w) {
-  double* p = sh + slot * 7 * kThreads + tid;
-  p[0 * kThreads] = w.d; p[1 * kThreads] = w.vx; p[2 * kThreads] = w.vy; p[3 * kThreads] = w.vz;
-  p[4 * kThreads] = w.p; p[5 * kThreads] = w.by; p[6 * kThreads] = w.bz;
+  double* p = sh + slot * 7 * NT + tid;
+  p[0 * NT] = w.d; p[1 * NT] = w.vx; p[2 * NT] = w.vy; p[3 * NT] = w.vz;
+  p[4 * NT] = w.p; p[5 * NT] = w.by; p[6 * NT] = w.bz;
 }
+template <int NT = kThreads>
 __device__ __forceinline__ Prim1 sh_load(const double* sh, int slot, int tid) {
-  const double* p = sh + slot * 7 * kThreads + tid;
+  const double* p = sh + slot * 7 * NT + tid;
   Prim1 w;
-  w.d = p[0 * kThreads]; w.vx = p[1 * kThreads]; w.vy = p[2 * kThreads]; w.vz = p[3 * kThreads];
-  w.p = p[4 * kThreads]; w.by = p[5 * kThreads]; w.bz = p[6 * kThreads];
+  w.d = p[0 * NT]; w.vx = p[1 * NT]; w.vy = p[2 * NT]; w.vz = p[3 * NT];
+  w.p = p[4 * NT]; w.by = p[5 * NT]; w.bz = p[6 * NT];
   return w;
 }
 
-template <int FLUX, bool TAPE = false>
+template <int FLUX, bool TAPE = false, int NT = kThreads>
 __device__ __forceinline__ void predict_y(const GridArgs& g, const PredictGeom& pg, int b) {
-  // slots 0..2: prims of rows k-1, k, k+1 (ring); slot 3: W_L of face k
-  __shared__ double sh[4 * 7 * kThreads];
+  // slots 0..2: prims of rows k-1, k, k+1 (ring); slot 3: W_L of face k.
+  // Above 128 threads the ring (4 x 7 x NT doubles) exceeds the 48 KB of
+  // static shared memory: the launch supplies it as dynamic shared memory.
+  double* sh;
+  if constexpr (NT <= 128) {
+    __shared__ double sh_static[4 * 7 * NT];
+    sh = sh_static;
+  } else {
+    extern __shared__ double sh_dynamic[];
+    sh = sh_dynamic;
+  }
   const StepState& st = *g.st;
   const int tid = threadIdx.x;
-  const int T = b * kThreads + tid;
+  const int T = b * NT + tid;
   if (T >= pg.ycols * pg.yseg) return;
   const int i = g.is - 2 + T % pg.ycols;
   const int ja = g.js - 1 + (T / pg.ycols) * g.ly;
   const int jb = min(ja + g.ly - 1, g.je + 2);
   const double* s = g.in;
 
-  sh_store(sh, 0, tid, prim_y(g, s, off(g, ja - 2, i)));
-  sh_store(sh, 1, tid, prim_y(g, s, off(g, ja - 1, i)));
+  sh_store<NT>(sh, 0, tid, prim_y(g, s, off(g, ja - 2, i)));
+  sh_store<NT>(sh, 1, tid, prim_y(g, s, off(g, ja - 1, i)));
   int r0 = 0;  // ring slot of row k-1
   for (int k = ja - 1; k <= jb; k++) {
     const long long o = off(g, k, i);
     const int r1 = r0 == 2 ? 0 : r0 + 1, r2 = r1 == 2 ? 0 : r1 + 1;
-    sh_store(sh, r2, tid, prim_y(g, s, o + g.pitch));
+    sh_store<NT>(sh, r2, tid, prim_y(g, s, o + g.pitch));
     Prim1 wln, wrt;
-    plm_cell(sh_load(sh, r0, tid), sh_load(sh, r1, tid), sh_load(sh, r2, tid), s[P_B2C * g.ps + o],
+    plm_cell(sh_load<NT>(sh, r0, tid), sh_load<NT>(sh, r1, tid), sh_load<NT>(sh, r2, tid), s[P_B2C * g.ps + o],
              st.dtodx2, g.eos, wln, wrt);
     // "MHD source terms" for 0.5*dt (src/__integrate_2d__.c:216-224)
     const double b2l = s[P_B2I * g.ps + o], b2r = s[P_B2I * g.ps + o + g.pitch];
@@ -212,7 +224,7 @@ __device__ __forceinline__ void predict_y(const GridArgs& g, const PredictGeom& 
     wrt.bz += st.hdt * src;
     if (k >= ja) {
       // step 2e (src/__integrate_2d__.c:233-241)
-      const Prim1 wl = sh_load(sh, 3, tid);
+      const Prim1 wl = sh_load<NT>(sh, 3, tid);
       const Cons1 ul = prim_to_cons(wl, b2l, g.eos);
       const Cons1 ur = prim_to_cons(wrt, b2l, g.eos);
       store_cons(g.scr + S_ULY * g.ps, g.ps, o, ul);
@@ -223,7 +235,7 @@ __device__ __forceinline__ void predict_y(const GridArgs& g, const PredictGeom& 
         store_prim(g.scr + T_WRTY * g.ps, g.ps, o, wrt);
       }
     }
-    sh_store(sh, 3, tid, wln);
+    sh_store<NT>(sh, 3, tid, wln);
     r0 = r1;
   }
 }
@@ -244,13 +256,13 @@ constexpr int kCorrectMinBlocks = ATHB_CORRECT_MIN_BLOCKS;
 // come first and the short role-X row segments (31 faces) last, so the
 // block scheduler ends the launch on small blocks instead of a tail of
 // marches.
-template <int FLUX, bool TAPE = false>
+template <int FLUX, bool TAPE = false, int NT = kThreads>
 __device__ __forceinline__ void predict_block(const GridArgs& g, const PredictGeom& pg, int b) {
   if (b < pg.ny_blocks) {
-    predict_y<FLUX, TAPE>(g, pg, b);
+    predict_y<FLUX, TAPE, NT>(g, pg, b);
   } else {
     b -= pg.ny_blocks;
-    predict_x<FLUX, TAPE>(g, b % pg.xseg, b / pg.xseg);
+    predict_x<FLUX, TAPE, NT>(g, b % pg.xseg, b / pg.xseg);
   }
 }
 
@@ -468,16 +480,16 @@ __device__ __forceinline__ void correct_e(const GridArgs& g, int t, int w) {
   g.scr[S_ECC * ps + o] = (B1c * M2 - B2c * M1) / d;
 }
 
-template <int FLUX>
+template <int FLUX, int NT = kThreads>
 __device__ __forceinline__ void correct_block(const GridArgs& g, const CorrectGeom& cg, int b) {
   if (b < cg.xb) {
-    const int t = b * kThreads + threadIdx.x;
+    const int t = b * NT + threadIdx.x;
     if (t < cg.xw * cg.xn) correct_x<FLUX>(g, t, cg.xw);
   } else if (b < cg.xb + cg.yb) {
-    const int t = (b - cg.xb) * kThreads + threadIdx.x;
+    const int t = (b - cg.xb) * NT + threadIdx.x;
     if (t < cg.yw * cg.yn) correct_y<FLUX>(g, t, cg.yw);
   } else {
-    const int t = (b - cg.xb - cg.yb) * kThreads + threadIdx.x;
+    const int t = (b - cg.xb - cg.yb) * NT + threadIdx.x;
     if (t < cg.ew * cg.en) correct_e(g, t, cg.ew);
   }
 }
@@ -506,9 +518,11 @@ __device__ __forceinline__ double cell_dti(double d, double m1, double m2, doubl
   return m;
 }
 
-// Block max of a non-negative double, then one atomicMax on its bit pattern.
+// Block max of a non-negative double, then one atomicMax on its bit pattern
+// (blocks of NT threads).
+template <int NT = kThreads>
 __device__ __forceinline__ void block_max_to(double v, unsigned long long* dst, int* flags) {
-  __shared__ double red[kThreads / 32];
+  __shared__ double red[NT / 32];
   if (!(v >= 0.0) || isinf(v)) { atomicOr(flags, kErrNonFinite); v = 0.0; }
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, d));
@@ -517,7 +531,7 @@ __device__ __forceinline__ void block_max_to(double v, unsigned long long* dst, 
   if (threadIdx.x == 0) {
     double m = red[0];
 #pragma unroll
-    for (int k = 1; k < kThreads / 32; k++) m = fmax(m, red[k]);
+    for (int k = 1; k < NT / 32; k++) m = fmax(m, red[k]);
     atomicMax(dst, (unsigned long long)__double_as_longlong(m));
   }
 }

@@ -324,6 +324,11 @@ void *athb_batch_stream(athb_batch *b);
 int athb_batch_set_ly(athb_batch *b, int k, int ly);
 int athb_batch_commit(athb_batch *b);
 int athb_batch_set_grid(athb_batch *b, int blocks);
+/* threads per work unit of the phased launches: 64, 128 (default) or 256;
+ * applied by athb_batch_commit; the persistent mode keeps 128.  Results do
+ * not depend on it.                                                         */
+int athb_batch_set_threads(athb_batch *b, int nt);
+int athb_batch_threads(const athb_batch *b);
 int athb_batch_grid(const athb_batch *b);
 /* per-phase time, accumulated in ms_out[6]: predict, emf (half step),
  * correct, emf (full step), update, ghost + finalize (persistent mode: block

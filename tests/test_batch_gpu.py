@@ -119,3 +119,41 @@ def test_hlle_batch_matches_reference(mode, tmp_path):
             assert refutil.mismatch_report(g.download()[0], planes, PLANES) == ""
             g.close()
     b.close()
+
+
+@pytest.mark.parametrize("nt", [64, 256])
+def test_threads_per_unit_give_the_same_bits(nt):
+    """64- and 256-thread work units (the phased launches' block size, which
+    the autotuner picks) give the 128-thread result bit for bit."""
+    items = _items()
+    want = Batch.from_problems(items)
+    assert want.threads == 128
+    want.run(10_000)
+    ref = [want.download(k) for k in range(want.n)]
+    want.close()
+    b = Batch.from_problems(items)
+    b.threads = nt
+    for k in range(b.n):
+        b.set_ly(k, 3 + 5 * k)
+    b.commit()
+    b.run(10_000)
+    for k in range(b.n):
+        planes, dt, t, n = b.download(k)
+        assert refutil.mismatch_report(ref[k][0], planes, PLANES) == ""
+        assert (dt, t, n) == ref[k][1:]
+    from athena_cuda_b200 import AthbError
+    with pytest.raises(AthbError, match="128-thread"):
+        b.mode = Batch.PERSISTENT
+    b.close()
+
+
+def test_autotuner_picks_threads_and_segments(tmp_path):
+    from athena_cuda_b200 import autotune
+
+    items = _items()
+    b = Batch.from_problems(items)
+    sizes = [(bl["grid"]["Nx1"], bl["grid"]["Nx2"]) for _, bl in items]
+    table = autotune.tune_batch(b, sizes, cache=tmp_path / "tune.json")
+    assert table["threads"] in autotune.NT_CANDIDATES and b.threads == table["threads"]
+    assert set(table["estimated_ms_per_launch_by_threads"]) == {"64", "128", "256"}
+    b.close()
