@@ -29,27 +29,27 @@ using namespace athb;
 
 namespace {
 
-// rows [j0, j0+nrows) of the 11 planes (sx wide, ghost columns included) <->
-// buf laid out [plane][row][sx]
-__global__ void __launch_bounds__(kThreads) k_rows_pack(const double* __restrict__ s, long long ps, int pitch, int sx,
-                                                       int j0, int nrows, double* __restrict__ buf) {
-  const long long per = (long long)nrows * sx, n = per * NSTATE;
+// the rectangle rows [j0, j0+nj) x columns [i0, i0+ni) of the 11 planes <->
+// buf laid out [plane][row][column]
+__global__ void __launch_bounds__(kThreads) k_rect_pack(const double* __restrict__ s, long long ps, int pitch, int i0,
+                                                       int ni, int j0, int nj, double* __restrict__ buf) {
+  const long long per = (long long)nj * ni, n = per * NSTATE;
   for (long long t = blockIdx.x * (long long)kThreads + threadIdx.x; t < n; t += (long long)gridDim.x * kThreads) {
     const int p = (int)(t / per);
     const long long r = t - p * per;
-    const int j = (int)(r / sx), i = (int)(r - (long long)j * sx);
-    buf[t] = s[p * ps + (long long)(j0 + j) * pitch + i];
+    const int j = (int)(r / ni), i = (int)(r - (long long)j * ni);
+    buf[t] = s[p * ps + (long long)(j0 + j) * pitch + i0 + i];
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_rows_unpack(double* __restrict__ s, long long ps, int pitch, int sx,
-                                                         int j0, int nrows, const double* __restrict__ buf) {
-  const long long per = (long long)nrows * sx, n = per * NSTATE;
+__global__ void __launch_bounds__(kThreads) k_rect_unpack(double* __restrict__ s, long long ps, int pitch, int i0,
+                                                         int ni, int j0, int nj, const double* __restrict__ buf) {
+  const long long per = (long long)nj * ni, n = per * NSTATE;
   for (long long t = blockIdx.x * (long long)kThreads + threadIdx.x; t < n; t += (long long)gridDim.x * kThreads) {
     const int p = (int)(t / per);
     const long long r = t - p * per;
-    const int j = (int)(r / sx), i = (int)(r - (long long)j * sx);
-    s[p * ps + (long long)(j0 + j) * pitch + i] = buf[t];
+    const int j = (int)(r / ni), i = (int)(r - (long long)j * ni);
+    s[p * ps + (long long)(j0 + j) * pitch + i0 + i] = buf[t];
   }
 }
 
@@ -68,26 +68,38 @@ int grid_of(long long n) {
   return (int)(b < 148LL * 8 ? (b < 1 ? 1 : b) : 148LL * 8);
 }
 
-int row_range_ok(const athb_ctx* c, int j0, int nrows) { return j0 >= 0 && nrows >= 1 && j0 + nrows <= c->sy; }
+int rect_ok(const athb_ctx* c, int i0, int ni, int j0, int nj) {
+  return i0 >= 0 && ni >= 1 && i0 + ni <= c->sx && j0 >= 0 && nj >= 1 && j0 + nj <= c->sy;
+}
 
 }  // namespace
 
-extern "C" int athb_rows_pack(athb_ctx* c, int j0, int nrows, double* dev) {
-  if (!c || !dev || !row_range_ok(c, j0, nrows)) return athb_fail(ATHB_ERR_ARG, "bad row range");
+extern "C" int athb_rect_pack(athb_ctx* c, int i0, int ni, int j0, int nj, double* dev) {
+  if (!c || !dev || !rect_ok(c, i0, ni, j0, nj)) return athb_fail(ATHB_ERR_ARG, "bad rectangle");
   CUDA_TRY(cudaSetDevice(c->cfg.device));
-  k_rows_pack<<<grid_of((long long)nrows * c->sx * NSTATE), kThreads, 0, c->stream>>>(
-      c->state[c->cur], c->ps, c->pitch, c->sx, j0, nrows, dev);
+  k_rect_pack<<<grid_of((long long)ni * nj * NSTATE), kThreads, 0, c->stream>>>(c->state[c->cur], c->ps, c->pitch,
+                                                                                i0, ni, j0, nj, dev);
   CUDA_TRY(cudaGetLastError());
   return ATHB_OK;
 }
 
-extern "C" int athb_rows_unpack(athb_ctx* c, int j0, int nrows, const double* dev) {
-  if (!c || !dev || !row_range_ok(c, j0, nrows)) return athb_fail(ATHB_ERR_ARG, "bad row range");
+extern "C" int athb_rect_unpack(athb_ctx* c, int i0, int ni, int j0, int nj, const double* dev) {
+  if (!c || !dev || !rect_ok(c, i0, ni, j0, nj)) return athb_fail(ATHB_ERR_ARG, "bad rectangle");
   CUDA_TRY(cudaSetDevice(c->cfg.device));
-  k_rows_unpack<<<grid_of((long long)nrows * c->sx * NSTATE), kThreads, 0, c->stream>>>(
-      c->state[c->cur], c->ps, c->pitch, c->sx, j0, nrows, dev);
+  k_rect_unpack<<<grid_of((long long)ni * nj * NSTATE), kThreads, 0, c->stream>>>(c->state[c->cur], c->ps, c->pitch,
+                                                                                  i0, ni, j0, nj, dev);
   CUDA_TRY(cudaGetLastError());
   return ATHB_OK;
+}
+
+extern "C" int athb_rows_pack(athb_ctx* c, int j0, int nrows, double* dev) {
+  if (!c) return athb_fail(ATHB_ERR_ARG, "null context");
+  return athb_rect_pack(c, 0, c->sx, j0, nrows, dev);
+}
+
+extern "C" int athb_rows_unpack(athb_ctx* c, int j0, int nrows, const double* dev) {
+  if (!c) return athb_fail(ATHB_ERR_ARG, "null context");
+  return athb_rect_unpack(c, 0, c->sx, j0, nrows, dev);
 }
 
 extern "C" int athb_max_dti_bits_device(athb_ctx* c, unsigned long long* dev) {

@@ -182,6 +182,11 @@ int athb_rows_put(athb_ctx *ctx, int j0, int nrows, const double *host);
  * through IPC mappings of every rank's word: n = ranks).                    */
 int athb_rows_pack(athb_ctx *ctx, int j0, int nrows, double *dev);
 int athb_rows_unpack(athb_ctx *ctx, int j0, int nrows, const double *dev);
+/* The same for the rectangle columns [i0, i0+ni) x rows [j0, j0+nj) (array
+ * indices, ghosts included), buffer [plane][row][column]: the x1 exchange of
+ * a 2D block decomposition.                                                 */
+int athb_rect_pack(athb_ctx *ctx, int i0, int ni, int j0, int nj, double *dev);
+int athb_rect_unpack(athb_ctx *ctx, int i0, int ni, int j0, int nj, const double *dev);
 int athb_max_dti_bits_device(athb_ctx *ctx, unsigned long long *dev);
 int athb_finish_step_device(athb_ctx *ctx, const unsigned long long *dev_bits, int n, int after_step);
 /* Device buffers shared between processes: cudaMalloc'd (zeroed) on the
