@@ -4,7 +4,7 @@ from __future__ import annotations
 
 import pytest
 
-from athena_cuda_b200.decomp import NG, neighbours, slab_rows, x2_sides
+from athena_cuda_b200.decomp import NG, block_neighbours, neighbours, slab_rows, x2_sides
 
 
 def test_slab_rows_cover_the_grid_once():
@@ -35,3 +35,25 @@ def test_transport_is_checked_before_any_device_work():
         SlabGrid(configs.blast(16, 16), "blast", 0, 2, transport="tcp")
     with pytest.raises(ValueError, match="at most"):
         SlabGrid(configs.blast(16, 16 * (MAX_RANKS + 1)), "blast", 0, MAX_RANKS + 1, transport="ipc")
+
+
+def test_block_neighbours_2d():
+    # 3 x 2 blocks, periodic in x1, walls in x2: rank = rx + 3 ry
+    nb = block_neighbours(4, 3, 2, True, False)      # rx = 1, ry = 1
+    assert nb[0] == (3, 5) and nb[1] == (1, None)
+    assert nb["sides1"] == 0 and nb["sides2"] == 2
+    nb = block_neighbours(0, 3, 2, True, False)
+    assert nb[0] == (2, 1) and nb[1] == (None, 3) and nb["sides2"] == 1
+    # one block across x1: its x1 ghosts are its own (periodic fill)
+    nb = block_neighbours(1, 1, 2, True, True)
+    assert nb[0] == (None, None) and nb["sides1"] == 3 and nb[1] == (0, 0) and nb["sides2"] == 0
+    # every low/high pair is mutual
+    for px, py in ((2, 2), (3, 2), (2, 3), (4, 1)):
+        for r in range(px * py):
+            nb = block_neighbours(r, px, py, True, True)
+            for d in (0, 1):
+                lo, hi = nb[d]
+                assert (lo is None) == (hi is None) == ((px, py)[d] == 1)
+                if lo is not None:
+                    assert block_neighbours(lo, px, py, True, True)[d][1] == r
+                    assert block_neighbours(hi, px, py, True, True)[d][0] == r

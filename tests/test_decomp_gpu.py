@@ -1,6 +1,6 @@
-"""A grid split over processes as x2 slabs (athena_cuda_b200/decomp.py) gives
-the single grid's state bit for bit: 2 and 3 ranks, periodic, outflow and
-reflecting x2 boundaries.  The ranks share this one GPU and exchange rows
+"""A grid split over processes as x2 slabs or px x py blocks
+(athena_cuda_b200/decomp.py) gives the single grid's state bit for bit: 2, 3,
+4 and 6 ranks, periodic, outflow, reflecting and mixed boundaries.  The ranks share this one GPU and exchange rows
 through host memory (transport "host", gloo) or through device buffers
 (transport "ipc": rows packed on the GPU and copied with cudaMemcpyAsync into
 the neighbours' CUDA-IPC-mapped receive buffers, the 1/dt maximum over device
@@ -20,10 +20,18 @@ import torch.multiprocessing as mp
 pytestmark = pytest.mark.gpu
 
 ROOT = Path(__file__).resolve().parent.parent
-CASES = {
-    "loop_periodic_2": ("field_loop", dict(nx1=48, nx2=36), 2, 20),
-    "blast_outflow_reflect_3": ("blast", dict(nx1=40, nx2=60, bc=(2, 2, 1, 2)), 3, 25),
-    "blast_periodic_3": ("blast", dict(nx1=30, nx2=45), 3, 25),
+CASES = {   # name: (problem, grid, px, py, steps)
+    "loop_periodic_2": ("field_loop", dict(nx1=48, nx2=36), 1, 2, 20),
+    "blast_outflow_reflect_3": ("blast", dict(nx1=40, nx2=60, bc=(2, 2, 1, 2)), 1, 3, 25),
+    "blast_periodic_3": ("blast", dict(nx1=30, nx2=45), 1, 3, 25),
+}
+# 2D blocks (ipc transport): periodic both ways, mixed physical boundaries,
+# uneven splits, a 2 x 1 row of blocks
+BLOCK_CASES = {
+    "loop_periodic_2x2": ("field_loop", dict(nx1=40, nx2=36), 2, 2, 20),
+    "blast_mixed_3x2": ("blast", dict(nx1=45, nx2=34, bc=(1, 2, 2, 1)), 3, 2, 25),
+    "blast_periodic_2x1": ("blast", dict(nx1=38, nx2=30), 2, 1, 25),
+    "blast_reflect_1x2_ipc": ("blast", dict(nx1=30, nx2=41, bc=(1, 1, 1, 1)), 1, 2, 25),
 }
 
 
@@ -41,18 +49,25 @@ def _free_port() -> int:
 
 
 def _rank(rank, ranks, port, name, transport, q):
+    return _run_rank(rank, ranks, port, {**CASES, **BLOCK_CASES}[name], transport, q)
+
+
+def _run_rank(rank, ranks, port, case, transport, q):
     import datetime
 
     import torch.distributed as dist
 
     sys.path.insert(0, str(ROOT))
-    from athena_cuda_b200.decomp import SlabGrid
+    from athena_cuda_b200.decomp import BlockGrid, SlabGrid
 
-    problem, kw, _, steps = CASES[name]
+    problem, kw, px, py, steps = case
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=ranks, timeout=datetime.timedelta(seconds=120))
     try:
-        s = SlabGrid(_blocks(problem, kw), problem, rank, ranks, transport=transport)
+        if px == 1 and transport == "host":
+            s = SlabGrid(_blocks(problem, kw), problem, rank, ranks, transport=transport)
+        else:
+            s = BlockGrid(_blocks(problem, kw), problem, rank, px, py, transport=transport)
         s.run(steps)
         per_iter_ms = 1e3 * s.exchange_s / max(1, s.iterations)
         full = s.gather()
@@ -64,12 +79,13 @@ def _rank(rank, ranks, port, name, transport, q):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("transport", ["host", "ipc"])
-@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("name,transport", [(n, t) for n in sorted(CASES) for t in ("host", "ipc")]
+                         + [(n, "ipc") for n in sorted(BLOCK_CASES)])
 def test_slabs_equal_single_grid(name, transport):
     from athena_cuda_b200 import Grid, Params
 
-    problem, kw, ranks, steps = CASES[name]
+    problem, kw, px, py, steps = {**CASES, **BLOCK_CASES}[name]
+    ranks = px * py
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
