@@ -36,6 +36,8 @@ using namespace athb;
 namespace {
 
 constexpr int kPhases = 6;
+constexpr int kPhasedGraphMinSteps = 32;
+constexpr int kRing256Bytes = 4 * 7 * 256 * (int)sizeof(double);   // predictor ring of 256-thread units
 constexpr long long kBarrierSpins = 20000000;  // x ~64 ns sleep: ~1-2 s
 constexpr int kBatchMinBlocks = 3;  // as k_predict: 168 registers per thread
 
@@ -461,6 +463,8 @@ static int upload_work(athb_batch* b) {
     CUDA_TRY(cudaGetLastError());
   }
   CUDA_TRY(cudaStreamSynchronize(b->stream));
+  // the phased step's graph holds the phase grid sizes of the old tables
+  if (b->mode == ATHB_BATCH_PHASED) drop_graph(b);
   return ATHB_OK;
 }
 
@@ -581,6 +585,13 @@ extern "C" int athb_batch_set_threads(athb_batch* b, int nt) {
   if (!b || (nt != 64 && nt != 128 && nt != 256)) return athb_fail(ATHB_ERR_ARG, "threads per unit: 64, 128 or 256");
   if (nt != kThreads && b->mode != ATHB_BATCH_PHASED)
     return athb_fail(ATHB_ERR_ARG, "the persistent mode runs 128-thread units");
+  if (nt == 256) {
+    CUDA_TRY(cudaSetDevice(b->device));
+    CUDA_TRY(cudaFuncSetAttribute(k_batch_phase<kFluxRoe, 0, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kRing256Bytes));
+    CUDA_TRY(cudaFuncSetAttribute(k_batch_phase<kFluxHlle, 0, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kRing256Bytes));
+  }
   b->nt = nt;
   for (int k = 0; k < b->n; k++) {
     InstGeom& I = b->geom[k];
@@ -722,16 +733,8 @@ template <int FLUX, int PH>
 static cudaError_t launch_phase(const athb_batch* b, const BatchDev& D) {
   if (b->phase_total[PH] > 0) {
     if (b->nt == 64) k_batch_phase<FLUX, PH, 64><<<b->phase_total[PH], 64, 0, b->stream>>>(D);
-    else if (b->nt == 256) {
-      // the predictor's role-Y ring in dynamic shared memory (see predict_y)
-      const int smem = PH == 0 ? 4 * 7 * 256 * (int)sizeof(double) : 0;
-      if (smem) {
-        cudaError_t e = cudaFuncSetAttribute(k_batch_phase<FLUX, PH, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             smem);
-        if (e != cudaSuccess) return e;
-      }
-      k_batch_phase<FLUX, PH, 256><<<b->phase_total[PH], 256, smem, b->stream>>>(D);
-    }
+    else if (b->nt == 256)   // the predictor's role-Y ring in dynamic shared memory (see predict_y)
+      k_batch_phase<FLUX, PH, 256><<<b->phase_total[PH], 256, PH == 0 ? kRing256Bytes : 0, b->stream>>>(D);
     else k_batch_phase<FLUX, PH, kThreads><<<b->phase_total[PH], kThreads, 0, b->stream>>>(D);
   }
   if (b->timing_on) k_stamp<<<1, 1, 0, b->stream>>>(b->timing, PH);
@@ -772,15 +775,18 @@ static int launch_step(athb_batch* b) {
   return ATHB_OK;
 }
 
-// Launch nsteps steps without synchronising (persistent: one cooperative
-// launch each, captured in a CUDA graph when CUDA accepts the capture; phased:
-// six launches each).
+// Launch nsteps steps without synchronising: one step (persistent: one
+// cooperative launch; phased: six launches) captured in a CUDA graph when
+// CUDA accepts the capture, then one graph launch per step.  The phased graph
+// is captured again whenever the work tables change (instances finishing),
+// and only for calls of at least kPhasedGraphMinSteps steps.
 extern "C" int athb_batch_run_async(athb_batch* b, int nsteps) {
   if (!b || nsteps < 0) return athb_fail(ATHB_ERR_ARG, "bad arguments");
   CUDA_TRY(cudaSetDevice(b->device));
-  // phased launches take their grid sizes from the active set, which changes
-  // as instances finish: launched directly (six launches a step)
-  if (b->mode == ATHB_BATCH_PERSISTENT && !b->graph && !b->graph_tried) {
+  // a phased graph is only worth capturing for a run of steps long enough to
+  // amortise it (its phase sizes change whenever an instance finishes)
+  const bool capture = b->mode == ATHB_BATCH_PERSISTENT || nsteps >= kPhasedGraphMinSteps;
+  if (capture && !b->graph && !b->graph_tried) {
     b->graph_tried = true;
     cudaGraph_t graph = nullptr;
     if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
@@ -794,7 +800,7 @@ extern "C" int athb_batch_run_async(athb_batch* b, int nsteps) {
     }
   }
   for (int s = 0; s < nsteps; s++) {
-    if (b->mode == ATHB_BATCH_PERSISTENT && b->graph) CUDA_TRY(cudaGraphLaunch(b->graph, b->stream));
+    if (b->graph) CUDA_TRY(cudaGraphLaunch(b->graph, b->stream));
     else { int rc = launch_step(b); if (rc) return rc; }
   }
   return ATHB_OK;
