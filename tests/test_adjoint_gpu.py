@@ -16,6 +16,7 @@ athb_adjoint_gradient through the C ABI).
 """
 from __future__ import annotations
 
+import os
 import subprocess
 import tempfile
 from pathlib import Path
@@ -185,7 +186,7 @@ def test_field_loop_256_finite_differences_of_reference(tmp_path):
         assert abs(ad[k] - med) <= max(abs(v - med) for v in vals) + 1e-3 * abs(med), sweep[-1]
     report += "\n" + "\n".join(sweep)
     print(report)
-    out = Path("gpurun_out") if Path("gpurun_out").is_dir() else Path(tempfile.gettempdir())
+    out = Path(os.environ.get("ATHB_REPORT_DIR", tempfile.gettempdir()))
     (out / "athb_fd_report.txt").write_text(report + "\n")
     assert sorted(r for _, _, _, r in rows)[len(rows) // 2] <= 1e-2, report
 
