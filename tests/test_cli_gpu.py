@@ -178,3 +178,29 @@ def test_cli_takes_problem_from_comment_config(tmp_path):
         assert r.returncode == 0, r.stderr
         outs[name] = (_cycles(r.stdout), _files(d))
     assert outs["p"] == outs["comment"] and outs["p"][1]
+
+
+@pytest.mark.parametrize("problem,blocks,expr,usr,palette", [
+    ("blast", configs.blast(40, 30), "P", False, "jh_colors"),
+    ("field_loop", configs.field_loop(32, 24), "J3", True, "heat"),
+])
+def test_output_ppm_api_matches_reference_main(problem, blocks, expr, usr, palette, tmp_path):
+    """athb_output_ppm called through the Python binding on the initial state
+    writes the file the reference main program writes at t = 0."""
+    from athena_cuda_b200 import Grid, load_palette
+
+    out = {"out_fmt": "ppm", "out": expr, "dt": 10.0, "palette": palette, "id": "img"}
+    if usr:
+        out["usr_expr_flag"] = 1
+    blocks = _outputs(blocks, [out])
+    blocks["time"]["nlim"] = 1   # the output at t = 0, written before the one step
+    ath = write_athinput(tmp_path / "athinput", blocks)
+    runs = _run_both(problem, ath, [], tmp_path)
+    name = f"{blocks['job']['problem_id']}.0000.img.ppm"
+    want = runs["ref"][1][name]
+    g = Grid.from_athinput(ath, problem)
+    rgb = load_palette(PALETTES, palette)
+    gmin, gmax = g.output_ppm(tmp_path / "api.ppm", expr, usr_expr=usr, rgb=rgb)
+    g.close()
+    assert (tmp_path / "api.ppm").read_bytes() == want
+    assert gmin <= gmax

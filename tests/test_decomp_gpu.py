@@ -49,7 +49,7 @@ def _free_port() -> int:
 
 
 def _rank(rank, ranks, port, name, transport, q):
-    return _run_rank(rank, ranks, port, {**CASES, **BLOCK_CASES}[name], transport, q)
+    return _run_rank(rank, ranks, port, {**CASES, **BLOCK_CASES, **NCCL_CASES}[name], transport, q)
 
 
 def _run_rank(rank, ranks, port, case, transport, q):
@@ -62,7 +62,12 @@ def _run_rank(rank, ranks, port, case, transport, q):
 
     problem, kw, px, py, steps = case
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
-    dist.init_process_group("gloo", rank=rank, world_size=ranks, timeout=datetime.timedelta(seconds=120))
+    if transport == "nccl":
+        import torch
+
+        torch.cuda.set_device(0)
+    dist.init_process_group("nccl" if transport == "nccl" else "gloo", rank=rank, world_size=ranks,
+                            timeout=datetime.timedelta(seconds=120))
     try:
         if px == 1 and transport == "host":
             s = SlabGrid(_blocks(problem, kw), problem, rank, ranks, transport=transport)
@@ -79,12 +84,18 @@ def _run_rank(rank, ranks, port, case, transport, q):
         dist.destroy_process_group()
 
 
+# the NCCL transport needs one GPU per rank; on one GPU it runs as one rank,
+# which exercises its device maximum (a device word all-reduced by NCCL on the
+# grid's stream) but no exchange
+NCCL_CASES = {"loop_nccl_1": ("field_loop", dict(nx1=40, nx2=36), 1, 1, 15)}
+
+
 @pytest.mark.parametrize("name,transport", [(n, t) for n in sorted(CASES) for t in ("host", "ipc")]
-                         + [(n, "ipc") for n in sorted(BLOCK_CASES)])
+                         + [(n, "ipc") for n in sorted(BLOCK_CASES)] + [(n, "nccl") for n in NCCL_CASES])
 def test_slabs_equal_single_grid(name, transport):
     from athena_cuda_b200 import Grid, Params
 
-    problem, kw, px, py, steps = {**CASES, **BLOCK_CASES}[name]
+    problem, kw, px, py, steps = {**CASES, **BLOCK_CASES, **NCCL_CASES}[name]
     ranks = px * py
     ctx = mp.get_context("spawn")
     q = ctx.Queue()

@@ -153,3 +153,17 @@ def test_batch_cpaw2d_generator_matches_grid_device_generator():
         assert x[1:] == y[1:]
         g.close()
     b.close()
+
+
+@pytest.mark.parametrize("name,blocks", CASES[::2], ids=["blast", "field_loop"])
+def test_generate_device_equals_generate(name, blocks):
+    """athb_generate_device forms blast and the field loop exactly as
+    athb_generate does (both on the GPU, bit-identical to the host)."""
+    p = Params.from_blocks(blocks)
+    a, b = Grid.create(p.config()), Grid.create(p.config())
+    a.generate(name, p)
+    b.generate_device(name, p)
+    x, y = a.download(), b.download()
+    assert np.array_equal(x[0], y[0]) and x[1:] == y[1:]
+    a.close()
+    b.close()
