@@ -122,3 +122,33 @@ def test_reference_palettes_as_text():
         pytest.skip("reference palettes not available")
     for name in ("rainbow", "jh_colors", "step8", "step32", "idl1", "idl2", "heat"):
         np.testing.assert_array_equal(load_palette(pal, name), load_palette(h, name), err_msg=name)
+
+
+def test_null_handles_are_rejected_without_touching_a_gpu():
+    """The C ABI reports bad arguments with ATHB_ERR_ARG (1) and a message
+    instead of crashing; these checks run before any CUDA call."""
+    L = ctypes.CDLL(str(LIB_PATH))   # a handle of its own: no argtypes set
+    P = ctypes.c_void_p
+    buf = (ctypes.c_double * 16)()
+    checks = {
+        "athb_rect_pack": (None, 0, 4, 0, 4, ctypes.cast(buf, P)),
+        "athb_rect_unpack": (None, 0, 4, 0, 4, ctypes.cast(buf, P)),
+        "athb_rows_pack": (None, 0, 4, ctypes.cast(buf, P)),
+        "athb_finish_step_device": (None, ctypes.cast(buf, P), 1, 1),
+        "athb_max_dti_bits_device": (None, ctypes.cast(buf, P)),
+        "athb_copy_async": (None, ctypes.cast(buf, P), ctypes.cast(buf, P), ctypes.c_ulonglong(8)),
+        "athb_batch_set_threads": (None, 64),
+        "athb_adjoint_keep_workspace": (None, 1),
+        "athb_cpaw2d_errors": (None, ctypes.cast(buf, P)),
+        "athb_generate_device": (None, b"blast", None),
+    }
+    for name, args in checks.items():
+        f = getattr(L, name)
+        f.restype = ctypes.c_int
+        assert f(*args) == 1, name
+        L.athb_last_error.restype = ctypes.c_char_p
+        assert L.athb_last_error(), name
+    out = np.zeros(768, dtype=np.float32)
+    L.athb_palette_load.restype = ctypes.c_int
+    assert L.athb_palette_load(b"/nonexistent/palette.h", b"rainbow",
+                               out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))) == 7   # ATHB_ERR_IO
