@@ -174,6 +174,11 @@ class BlockGrid:
         self.j0, self.ny = self.rows[self.ry]
         per1 = gcfg.bc_ix1 == 4 and gcfg.bc_ox1 == 4
         per2 = gcfg.bc_ix2 == 4 and gcfg.bc_ox2 == 4
+        # a periodic side needs the far end's cells: only both sides periodic
+        # (a ring) or neither can be split
+        for n, a, b in ((px, gcfg.bc_ix1, gcfg.bc_ox1), (py, gcfg.bc_ix2, gcfg.bc_ox2)):
+            if n > 1 and (a == 4) != (b == 4):
+                raise ValueError("a direction split over several ranks is periodic on both sides or on neither")
         nb = block_neighbours(rank, px, py, per1, per2)
         self.nbr = {X1: nb[X1], X2: nb[X2]}   # per direction: (low side, high side) ranks
         self.sides1, self.sides2 = nb["sides1"], nb["sides2"]

@@ -57,3 +57,11 @@ def test_block_neighbours_2d():
                 if lo is not None:
                     assert block_neighbours(lo, px, py, True, True)[d][1] == r
                     assert block_neighbours(hi, px, py, True, True)[d][0] == r
+
+
+def test_one_sided_periodic_direction_is_not_split():
+    from athena_cuda_b200 import configs
+    from athena_cuda_b200.decomp import BlockGrid
+
+    with pytest.raises(ValueError, match="periodic on both sides"):
+        BlockGrid(configs.blast(32, 32, bc=(2, 4, 4, 4)), "blast", 0, 2, 1, transport="ipc")

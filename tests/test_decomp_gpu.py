@@ -32,6 +32,8 @@ BLOCK_CASES = {
     "blast_mixed_3x2": ("blast", dict(nx1=45, nx2=34, bc=(1, 2, 2, 1)), 3, 2, 25),
     "blast_periodic_2x1": ("blast", dict(nx1=38, nx2=30), 2, 1, 25),
     "blast_reflect_1x2_ipc": ("blast", dict(nx1=30, nx2=41, bc=(1, 1, 1, 1)), 1, 2, 25),
+    "blast_hlle_2x2": ("blast", dict(nx1=64, nx2=48, bc=(2, 2, 4, 4), flux="hlle"), 2, 2, 30),
+    "loop_128x96_2x2": ("field_loop", dict(nx1=128, nx2=96), 2, 2, 40),
 }
 
 
