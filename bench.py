@@ -54,10 +54,11 @@ OPS_PER_ZC = {
 }
 OPS_STEP = sum(OPS_PER_ZC.values())
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
-# dominant kernels from one ncu capture of the 1024x1024 field loop
-# (profiles/k_predict_k_correct_k_update_field_loop_1024.md), scaled to
-# 2048x2048 by the cell ratio 4.  Applies to the 2048x2048 default workload.
-TRAFFIC_1024 = {"predict": 504.57e6, "correct": 722.01e6, "update_cfl": 237.09e6}
+# dominant kernels from single-kernel ncu captures of the 1024x1024 field loop
+# (profiles/k_predict_field_loop_1024.md, k_correct_k_update_field_loop_1024.md),
+# scaled to 2048x2048 by the cell ratio 4.  Applies to the 2048x2048 default
+# workload.
+TRAFFIC_1024 = {"predict": 508.49e6, "correct": 725.48e6, "update_cfl": 244.51e6}
 
 
 def parse():
