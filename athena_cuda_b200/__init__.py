@@ -130,6 +130,7 @@ def lib() -> C.CDLL:
             "athb_host_free": (None, [P]),
             "athb_tlm_run": (I, [P, I, dp, dp, dp, dp]),
             "athb_adjoint_keep_workspace": (I, [P, I]),
+            "athb_adjoint_vjp": (I, [P, I, C.c_longlong, dp, dp, dp, C.POINTER(AdjointStats)]),
             "athb_adjoint_gradient": (I, [P, I, C.c_longlong, dp, dp, C.POINTER(AdjointStats)]),
         }
         for name, (res, args) in sig.items():
@@ -330,6 +331,19 @@ class Grid:
         J = C.c_double()
         st = AdjointStats()
         _check(lib().athb_adjoint_gradient(self._h, nsteps, snapshot_bytes, C.byref(J), _dp(g), C.byref(st)))
+        stats = {k: getattr(st, k) for k, _ in AdjointStats._fields_}
+        return J.value, g, stats
+
+    def adjoint_vjp(self, nsteps: int, seed: np.ndarray, snapshot_bytes: int = 0):
+        """Adjoint of nsteps iterations for any objective of the final state:
+        seed = dJ/dS^N (state layout); returns (<seed, S^N>,
+        (dS^N/dS^0)^T seed, stats)."""
+        seed = np.ascontiguousarray(seed, dtype=np.float64)
+        assert seed.shape == (NPLANES, self.sy, self.sx)
+        g = np.empty((NPLANES, self.sy, self.sx))
+        J = C.c_double()
+        st = AdjointStats()
+        _check(lib().athb_adjoint_vjp(self._h, nsteps, snapshot_bytes, _dp(seed), C.byref(J), _dp(g), C.byref(st)))
         stats = {k: getattr(st, k) for k, _ in AdjointStats._fields_}
         return J.value, g, stats
 

@@ -158,6 +158,25 @@ struct ObjFn {
   }
 };
 
+// <seed, S> per cell: the 11 planes of an interior cell in plane order, then
+// the outer faces B1i(ie+1) and B2i(je+1) on the last column and row (the
+// entries a step writes; the seed is zero elsewhere).
+struct SeedDotFn {
+  const double* s;
+  const double* seed;
+  double* out;
+  long long ps;
+  int pitch, ie, je;
+  ATHB_MEM void operator()(int j, int i) const {
+    const long long o = (long long)j * pitch + i;
+    double v = 0.0;
+    for (int p = 0; p < NSTATE; p++) v += seed[p * ps + o] * s[p * ps + o];
+    if (i == ie) v += seed[P_B1I * ps + o + 1] * s[P_B1I * ps + o + 1];
+    if (j == je) v += seed[P_B2I * ps + o + pitch] * s[P_B2I * ps + o + pitch];
+    out[o] = v;
+  }
+};
+
 // dt after a forward step (value form for the records; T = Dual carries the
 // tangent): time, the rule, the clamp.  cf holds the next step's factors.
 template <class T> struct DtNextFn {
@@ -485,6 +504,10 @@ template <class Exec> struct AdjointDriver {
     return x.ok() ? 0 : -1;
   }
 
+  // a given cotangent of the final state (Exec memory, state layout, zero
+  // outside the entries a step writes), or null for the magnetic energy
+  const double* seed = nullptr;
+
   void objective(const double* s, const double* ds) {
     double* tmp = tape;   // any plane-sized scratch: the tape's first plane is free after the step
     x.items(interior(), ObjFn{s, nullptr, tmp, G.ps, G.pitch, 0});
@@ -674,10 +697,18 @@ template <class Exec> struct AdjointDriver {
         cur = c2;
       }
     }
-    // seed: dJ/dS^M
+    // seed: dJ/dS^M (the magnetic energy's, or a given cotangent of S^M,
+    // whose objective is then J = <seed, S^M>)
     lc = 0;
     x.zero(lam[0], state_doubles());
-    x.items(interior(), ObjFn{S[cur], nullptr, lam[0], G.ps, G.pitch, 2});
+    if (seed) {
+      x.copy(lam[0], seed, state_doubles());
+      double* tmp = tape;
+      x.items(interior(), SeedDotFn{S[cur], seed, tmp, G.ps, G.pitch, G.ie, G.je});
+      x.sum(tmp, interior(), G.pitch, &sc->J);
+    } else {
+      x.items(interior(), ObjFn{S[cur], nullptr, lam[0], G.ps, G.pitch, 2});
+    }
     x.zero_bytes(&sc->lrule, sizeof(double));
     x.zero_bytes(&sc->ltime, sizeof(double));
     if (tapes && M > 0) {

@@ -418,8 +418,10 @@ extern "C" int athb_tlm_run(athb_ctx* ctx, int nsteps, const double* dstate0, do
   return ATHB_OK;
 }
 
-extern "C" int athb_adjoint_gradient(athb_ctx* ctx, int nsteps, long long snapshot_bytes, double* J, double* grad,
-                                     athb_adjoint_stats* stats) {
+namespace {
+
+int adjoint_impl(athb_ctx* ctx, int nsteps, long long snapshot_bytes, const double* seed_host, double* J,
+                 double* grad, athb_adjoint_stats* stats) {
   if (!ctx || nsteps < 0) return athb_fail(ATHB_ERR_ARG, "athb_adjoint_gradient: bad arguments");
   CUDA_TRY(cudaSetDevice(ctx->cfg.device));
   const auto t0 = std::chrono::steady_clock::now();
@@ -431,6 +433,17 @@ extern "C" int athb_adjoint_gradient(athb_ctx* ctx, int nsteps, long long snapsh
   x.redm = (MaxLoc*)x.alloc_bytes(sizeof(MaxLoc) * kRedBlocks);
   x.st = (StepState*)x.alloc_bytes(sizeof(StepState));
   if (d.setup(nsteps, false)) return finish(x, "athb_adjoint_gradient: workspace");
+  if (seed_host) {   // the cotangent of S^N, on the entries a step writes
+    std::vector<double> h((size_t)NSTATE * ctx->sy * ctx->sx);
+    std::copy(seed_host, seed_host + h.size(), h.begin());
+    interior_only(ctx, h);
+    double* dseed = x.alloc(d.state_doubles());
+    if (!x.ok()) return finish(x, "athb_adjoint_vjp: seed");
+    x.zero(dseed, d.state_doubles());
+    x.note(planes_h2d(ctx, dseed, h.data(), x.s));
+    x.note(cudaStreamSynchronize(x.s));   // h is freed at the end of this block
+    d.seed = dseed;
+  }
   // snapshot slots: as many as the budget allows, at most one per step
   const size_t sbytes = sizeof(double) * d.state_doubles();
   long long budget = snapshot_bytes;
@@ -471,6 +484,19 @@ extern "C" int athb_adjoint_gradient(athb_ctx* ctx, int nsteps, long long snapsh
     stats->tape_mode = d.tapes != nullptr;
   }
   return ATHB_OK;
+}
+
+}  // namespace
+
+extern "C" int athb_adjoint_gradient(athb_ctx* ctx, int nsteps, long long snapshot_bytes, double* J, double* grad,
+                                     athb_adjoint_stats* stats) {
+  return adjoint_impl(ctx, nsteps, snapshot_bytes, nullptr, J, grad, stats);
+}
+
+extern "C" int athb_adjoint_vjp(athb_ctx* ctx, int nsteps, long long snapshot_bytes, const double* seed, double* J,
+                                double* grad, athb_adjoint_stats* stats) {
+  if (!seed) return athb_fail(ATHB_ERR_ARG, "athb_adjoint_vjp: null seed");
+  return adjoint_impl(ctx, nsteps, snapshot_bytes, seed, J, grad, stats);
 }
 
 // Keep (on != 0) the adjoint's device workspace between calls on this

@@ -396,6 +396,14 @@ int athb_tlm_run(athb_ctx *ctx, int nsteps, const double *dstate0, double *J, do
  * 1992) recomputes the fewest forward steps the room allows.                */
 int athb_adjoint_gradient(athb_ctx *ctx, int nsteps, long long snapshot_bytes, double *J, double *grad,
                           athb_adjoint_stats *stats);
+/* The same for any objective of the final state: seed is dJ/dS^N in the
+ * athb_upload layout (its entries on the cells a step writes are used: the
+ * interior, B1i to column ie+1, B2i to row je+1), grad = (dS^N/dS^0)^T seed
+ * and J = <seed, S^N>.  A user objective J(S^N) passes its gradient; with
+ * athb_tlm_run's final tangent state this gives any directional derivative.
+ * No reference counterpart.                                                 */
+int athb_adjoint_vjp(athb_ctx *ctx, int nsteps, long long snapshot_bytes, const double *seed, double *J,
+                     double *grad, athb_adjoint_stats *stats);
 /* Keep the device workspace of athb_adjoint_gradient / athb_tlm_run on this
  * context between calls (on = 1: a repeated call of the same size reuses it
  * instead of allocating and freeing up to most of the GPU's memory; the

@@ -30,6 +30,7 @@ def lib() -> C.CDLL:
         L.hc_forward.argtypes = [C.POINTER(Config), dp, C.c_int, dp, dp, dp]
         L.hc_tlm.argtypes = [C.POINTER(Config), dp, dp, C.c_int, dp, dp, dp, dp]
         L.hc_adjoint.argtypes = [C.POINTER(Config), dp, C.c_int, C.c_int, dp, dp, C.POINTER(C.c_longlong)]
+        L.hc_adjoint_seed.argtypes = [C.POINTER(Config), dp, dp, C.c_int, C.c_int, dp, dp]
         _lib = L
     return _lib
 
@@ -61,6 +62,17 @@ def adjoint(cfg, S0: np.ndarray, n: int, slots: int):
     J, adv = C.c_double(), C.c_longlong()
     steps = lib().hc_adjoint(C.byref(cfg), _p(S), n, slots, C.byref(J), _p(g), C.byref(adv))
     return J.value, g, steps, adv.value
+
+
+def adjoint_seed(cfg, S0: np.ndarray, seed: np.ndarray, n: int, slots: int):
+    """Adjoint seeded with a cotangent of the final state: (<seed, S^N>,
+    (dS^N/dS^0)^T seed, steps)."""
+    S = np.ascontiguousarray(S0, dtype=np.float64)
+    sd = np.ascontiguousarray(seed, dtype=np.float64)
+    g = np.zeros_like(S)
+    J = C.c_double()
+    steps = lib().hc_adjoint_seed(C.byref(cfg), _p(S), _p(sd), n, slots, C.byref(J), _p(g))
+    return J.value, g, steps
 
 
 def interior_direction(rng, cfg, planes=range(11)) -> np.ndarray:

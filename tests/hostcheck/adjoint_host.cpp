@@ -140,4 +140,26 @@ int hc_adjoint(const athb_config* cfg, const double* S0, int N, int nslot, doubl
   return steps;
 }
 
+// The adjoint seeded with a cotangent of the final state (state layout,
+// entries a step writes): J = <seed, S^N>, grad = (dS^N/dS^0)^T seed.
+int hc_adjoint_seed(const athb_config* cfg, const double* S0, const double* seed, int N, int nslot, double* J,
+                    double* grad) {
+  HostExec x;
+  AdjointDriver<HostExec> d(x, geom_of(cfg));
+  d.setup(N, false);
+  d.nslot = nslot < 1 ? 1 : nslot;
+  d.slots = x.alloc((size_t)d.nslot * d.state_doubles());
+  double* sd = x.alloc(d.state_doubles());
+  x.copy(sd, seed, d.state_doubles());
+  d.seed = sd;
+  x.copy(d.S[0], S0, d.state_doubles());
+  int lc = 0, steps = 0;
+  if (cfg->flux == ATHB_FLUX_HLLE) d.adjoint<kFluxHlle>(N, lc, steps); else d.adjoint<kFluxRoe>(N, lc, steps);
+  *J = d.sc->J;
+  x.copy(grad, d.lam[lc], d.state_doubles());
+  d.release();
+  x.release(sd);
+  return steps;
+}
+
 }  // extern "C"

@@ -146,3 +146,29 @@ def test_tangent_matches_oracle_finite_differences():
         Jpm.append(ah.objective(P, cfg))
     fd = (Jpm[0] - Jpm[1]) / (2 * eps)
     assert abs(fd - dJ) <= 1e-6 * abs(dJ), (fd, dJ)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_seeded_adjoint_is_the_transpose_of_the_tlm(name):
+    """athb_adjoint_vjp's code: for a random cotangent w of the final state,
+    <(dS^N/dS^0)^T w, d> = <w, dS^N(d)> (the TLM's final tangent state), and
+    J = <w, S^N>; the magnetic energy's seed (B1c, B2c) gives the plain
+    adjoint's gradient bit for bit."""
+    cfg, S0, n = _setup(name)
+    _, g0, steps, _ = ah.adjoint(cfg, S0, n, n + 1)
+    rng = np.random.default_rng(23)
+    w = ah.interior_direction(rng, cfg)
+    Jw, gw, steps_w = ah.adjoint_seed(cfg, S0, w, n, n + 1)
+    assert steps_w == steps
+    d = ah.interior_direction(rng, cfg)
+    _, _, SN, dSN = ah.tlm(cfg, S0, d, steps)
+    mask = ah.interior_direction(np.random.default_rng(0), cfg) != 0
+    assert abs(Jw - float(np.sum((w * SN)[mask]))) <= 1e-12 * float(np.sum(np.abs(w * SN)))
+    lhs, rhs = float(np.sum(gw * d)), float(np.sum((w * dSN)[mask]))
+    scale = max(float(np.sum(np.abs(gw * d))), float(np.sum(np.abs(w * dSN))))
+    assert abs(lhs - rhs) <= 1e-11 * scale, (name, lhs, rhs)
+    # the magnetic-energy seed reproduces the plain adjoint
+    seed = np.zeros_like(S0)
+    seed[5:7, 4:4 + cfg.nx2, 4:4 + cfg.nx1] = SN[5:7, 4:4 + cfg.nx2, 4:4 + cfg.nx1]
+    _, gm, _ = ah.adjoint_seed(cfg, S0, seed, n, 3)
+    assert np.array_equal(gm, g0)

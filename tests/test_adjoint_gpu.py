@@ -243,3 +243,24 @@ def test_kept_workspace_gives_the_same_gradient(tmp_path):
     J, g1, _ = g.adjoint_gradient(12)
     assert J == J0 and np.array_equal(g1, g0)
     g.close()
+
+
+@pytest.mark.parametrize("name", ["blast_mixed_bc", "field_loop"])
+def test_vjp_matches_host_and_transposes_the_tlm(name, tmp_path):
+    """athb_adjoint_vjp (a cotangent of the final state as the seed) on the
+    GPU: equal to the host build to the rounding of the reductions, and
+    <(dS^N/dS^0)^T w, d> = <w, dS^N(d)> with the GPU's tangent state."""
+    cfg, S0, g, n = _small(name, tmp_path)
+    rng = np.random.default_rng(31)
+    w = ah.interior_direction(rng, cfg)
+    J, grad, st = g.adjoint_vjp(n, w)
+    Jh, gh, steps = ah.adjoint_seed(cfg, S0, w, n, n + 1)
+    assert st["steps"] == steps
+    assert abs(J - Jh) <= 1e-12 * max(abs(Jh), 1e-300) + 1e-15
+    assert np.max(np.abs(grad - gh)) <= 1e-10 * np.max(np.abs(gh))
+    d = ah.interior_direction(rng, cfg)
+    _, _, dS = g.tlm(steps, d, want_state=True)
+    mask = ah.interior_direction(np.random.default_rng(0), cfg) != 0
+    lhs, rhs = float(np.sum(grad * d)), float(np.sum((w * dS)[mask]))
+    assert abs(lhs - rhs) <= 1e-11 * max(float(np.sum(np.abs(grad * d))), 1e-300), (lhs, rhs)
+    g.close()
