@@ -542,6 +542,36 @@ template <class Exec> struct AdjointDriver {
     return a;
   }
 
+  // The ghost fill of a state, reversed on its adjoint l: the ghost rows'
+  // adjoints added onto the rows they copy (x2), then the ghost columns'
+  // onto the columns they copy (x1), then the frame cleared.  Only rows and
+  // columns within kBand of an edge are copied by a ghost (periodic wraps
+  // reach 4 cells in, reflection 4, outflow 1), so the passes visit those
+  // bands alone; every target cell adds the same terms in the same order.
+  void fold_ghosts(double* l) {
+    const GhostGeom gg = ghost_geom();
+    constexpr int kBand = kNghostA + 2;
+    const int is = G.is, ie = G.ie, js = G.js, je = G.je;
+    if (2 * kBand >= je + 2 - js) {
+      x.items(GenRange{0, G.sx - 1, js, je + 1}, FoldFn{l, G.ps, G.pitch, gg, 2});
+    } else {
+      x.items(GenRange{0, G.sx - 1, js, js + kBand - 1}, FoldFn{l, G.ps, G.pitch, gg, 2});
+      x.items(GenRange{0, G.sx - 1, je + 2 - kBand, je + 1}, FoldFn{l, G.ps, G.pitch, gg, 2});
+    }
+    if (2 * kBand >= ie + 2 - is) {
+      x.items(GenRange{is, ie + 1, js, je + 1}, FoldFn{l, G.ps, G.pitch, gg, 1});
+    } else {
+      x.items(GenRange{is, is + kBand - 1, js, je + 1}, FoldFn{l, G.ps, G.pitch, gg, 1});
+      x.items(GenRange{ie + 2 - kBand, ie + 1, js, je + 1}, FoldFn{l, G.ps, G.pitch, gg, 1});
+    }
+    // the frame: rows below js and above je (B2i's row je+1 is kept by the
+    // functor), the columns left of is and right of ie on the rows between
+    x.items(GenRange{0, G.sx - 1, 0, js - 1}, FoldFn{l, G.ps, G.pitch, gg, 0});
+    x.items(GenRange{0, G.sx - 1, je + 1, G.sy - 1}, FoldFn{l, G.ps, G.pitch, gg, 0});
+    x.items(GenRange{0, is - 1, js, je}, FoldFn{l, G.ps, G.pitch, gg, 0});
+    x.items(GenRange{ie + 1, G.sx - 1, js, je}, FoldFn{l, G.ps, G.pitch, gg, 0});
+  }
+
   // Reverse step n: S^n in S[cur].  lam[lc] holds the adjoint of S^{n+1}
   // (folded); on return lam[lc^1] holds that of S^n (folded), lc flipped.
   template <int FLUX> void reverse_step(int cur, int n, int N, int& lc, const std::vector<StepRec>& hrec) {
@@ -586,10 +616,7 @@ template <class Exec> struct AdjointDriver {
     x.items(GenRange{is - 3, ie + 3, js - 2, je + 2}, AdjFn<R_PRIMX, FLUX>{a});
     x.items(GenRange{is - 2, ie + 2, js - 3, je + 3}, AdjFn<R_PRIMY, FLUX>{a});
     // the ghost fill of S^n, reversed: x2 rows, then x1 columns, then clear
-    const GhostGeom gg = ghost_geom();
-    x.items(GenRange{0, G.sx - 1, G.js, G.je + 1}, FoldFn{lin, G.ps, G.pitch, gg, 2});
-    x.items(GenRange{G.is, G.ie + 1, G.js, G.je + 1}, FoldFn{lin, G.ps, G.pitch, gg, 1});
-    x.items(full(), FoldFn{lin, G.ps, G.pitch, gg, 0});
+    fold_ghosts(lin);
     // dt^n
     x.sum(adj + (long long)A_DT * G.ps, GenRange{is - 3, ie + 3, js - 3, je + 3}, G.pitch, &sc->dtsum);
     x.single(DtStepAdjFn{sc, rec, n, n + 1 == N ? 1 : 0});
